@@ -1,0 +1,339 @@
+"""Throughput of the entropy-stable flux-differencing RHS on B200.
+
+Workload (one "step" = one LSRK-45 time step = 5 stages x {vol, surf, update}):
+  3D Taylor-Green vortex on affine tetrahedra (Euler3Daffine kernels), FP64,
+  periodic [-pi,pi]^3, 16^3 hexes x 6 tets = 24576 elements, N = 3,
+  gamma = 1.4, CFL 0.5.  Synthetic: the mesh and the initial state are
+  generated here (no external data).
+Metric: FP64 DOF*stages/s, DOF = K * Np per field (Np = 20, Nfields = 5).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl ours       the CUDA library through its C ABI; `value` is timed with
+                  CUDA events around K graph-replayed time steps with the state
+                  resident in HBM (working set ~0.3 GB > L2); `e2e` is the
+                  user-level host-buffer solve (wadg_app_solve_host: H2D of the
+                  stage-0 state from pinned memory, the config's 100 time
+                  steps, D2H of Q).  Multi-GPU: independent replicas (the path
+                  has no data exchange), max time over ranks.
+--impl reference  the reference's own kernels compiled from its OKL sources
+                  (oracle/_ref, OpenMP over all host cores; the C restatement
+                  when oracle/_ref is absent) on the same workload; rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 DOF*stages/s at N=3 (3D affine-tet Taylor-Green, Euler3Daffine RHS)"
+UNIT = "DOF*stages/s"
+WORKLOAD = "taylor_green_3d_affine_N3_K24576"
+NHEX, N, CFL, E2E_STEPS = 16, 3, 0.5, 100
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def build_workload():
+    from scratch_wadge_b200 import ic as IC
+    from scratch_wadge_b200 import mesh as M
+    geo = M.build_geometry(M.periodic_cube(NHEX), N)
+    Q, rhsQ, Qf, resQ = IC.stage0(geo, IC.initial_state(geo, "taylor_green"))
+    dt, _ = IC.time_step(geo, CFL, N, nsteps=E2E_STEPS)
+    return geo, dict(Q=Q, rhsQ=rhsQ, Qf=Qf, resQ=resQ), dt
+
+
+def config_dict(geo, n_gpus):
+    return {"workload": WORKLOAD, "mesh": f"periodic [-pi,pi]^3, {NHEX}^3 hexes x 6 tets",
+            "K": geo.K, "N": N, "Np": geo.ops.Np, "Nq": geo.ops.Nq, "NfqNf": geo.ops.NfqNf,
+            "Nfields": 5, "dofs_per_field": geo.K * geo.ops.Np,
+            "step": "one LSRK-45 time step (5 stages x vol+surf+update)",
+            "l2": "inputs larger than L2 (state + geometry ~0.3 GB per replica)",
+            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        mx = max(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def ncu_traffic():
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_impl():
+    """The CPU implementation of the path: the reference's kernels compiled
+    from its sources when available, else the oracle's C restatement."""
+    from oracle import pyoracle as O
+    if O.reference_available(3, N):
+        return O.Reference, "reference"
+    return O.Port, "port"
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def time_cpu(geo, st0, dt, steps):
+    """Wall time of `steps` full time steps of the CPU implementation."""
+    cls, kind = cpu_impl()
+    impl = cls(geo.ops, False)
+    st = {k: v.copy() for k, v in st0.items()}
+    st["rhsQf"] = np.zeros_like(st["Qf"])
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        impl.step(geo, dt, st)
+    return time.perf_counter() - t0, kind
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+    geo, st0, dt = build_workload()
+    dofs = geo.K * geo.ops.Np
+    _, kind = cpu_impl()
+    # each step: one full time step of the whole workload (5 stages)
+    if args.warmup > 0:
+        time_cpu(geo, st0, dt, min(args.warmup, 1))
+    sec, _ = time_cpu(geo, st0, dt, args.steps)
+    v = dofs * 5 * args.steps / sec
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(geo, 1),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+                             "kind": kind,
+                             "sample": f"{args.steps} full LSRK-45 time steps of the whole workload "
+                                       f"(K={geo.K}), OpenMP over elements"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from scratch_wadge_b200 import build as B
+    from scratch_wadge_b200 import capi
+    from scratch_wadge_b200 import roofline as RF
+    B.build()
+
+    geo, st0, dt = build_workload()
+    ops = geo.ops
+    K, Nq, NfqNf, Np = geo.K, ops.Nq, ops.NfqNf, ops.Np
+    dofs = K * Np
+    stream = torch.cuda.Stream()
+    app = capi.App(geo, curved=False, stream=stream.cuda_stream)
+    app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also captures the time-step graph)
+    app.rk_run(dt, max(args.warmup, 1), graph=True)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        app.rk_run(dt, args.steps, graph=True)
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    clocks = clk.summary()
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * dofs * 5 * args.steps / (ms * 1e-3)
+
+    # per-kernel device times (CUDA events around each launch, app stream)
+    nst = 20
+    kms = app.time_kernels(dt, nst)
+    vol_ms, surf_ms, upd_ms = (x / nst for x in kms)
+    fl = RF.vol_flops_per_element(3, Nq, NfqNf, False) * K
+    probe = fp64_peak(stream)
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    achieved = fl / (vol_ms * 1e-3) / 1e12
+    traffic = ncu_traffic().get("vol_3d_affine_N3_K24576")
+    roof = {"kernel": "euler_vol_3d (volume flux differencing)", "bound": "fp64",
+            "achieved": achieved, "peak": probe, "unit": "TFLOP/s", "frac": achieved / probe,
+            "traffic": traffic,
+            "peak_source": "measured in-run: FP64 FMA probe (wadg_probe_fp64_fma)",
+            "algorithmic_flops_per_launch": fl, "launch_ms": vol_ms,
+            "flops_per_element": RF.vol_flops_per_element(3, Nq, NfqNf, False),
+            "pairs_per_element": RF.pairs_per_element(Nq, NfqNf)}
+    sb = RF.surf_bytes_per_element(3, Nq, NfqNf) * K
+    ub = RF.update_bytes_per_element(3, Nq, NfqNf) * K
+    hbm_kernels = {
+        "euler_surf_3d": {"launch_ms": surf_ms, "achieved_gbs": sb / (surf_ms * 1e-3) / 1e9,
+                          "frac": (sb / (surf_ms * 1e-3) / 1e9) / hbm if hbm else None},
+        "euler_update_3d": {"launch_ms": upd_ms, "achieved_gbs": ub / (upd_ms * 1e-3) / 1e9,
+                            "frac": (ub / (upd_ms * 1e-3) / 1e9) / hbm if hbm else None},
+        "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)" if hbm else None}
+
+    # end to end through the user-level host-buffer call
+    pin = {k: torch.from_numpy(v).pin_memory() for k, v in st0.items()}
+    Qout = torch.empty(pin["Q"].shape, dtype=torch.float64).pin_memory()
+    host = {k: v.numpy() for k, v in pin.items()}
+    qo = Qout.numpy()
+    app.solve_host(host["Q"], host["rhsQ"], host["Qf"], dt, 2, resQ0=host["resQ"], out=qo)  # warm
+    barrier()
+    e2e_calls = max(1, args.e2e_calls)
+    t0 = time.perf_counter()
+    for _ in range(e2e_calls):
+        app.solve_host(host["Q"], host["rhsQ"], host["Qf"], dt, E2E_STEPS, resQ0=host["resQ"], out=qo)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_v = ws * dofs * 5 * E2E_STEPS * e2e_calls / e2e_s
+    h2d = sum(v.nbytes for v in host.values())
+    d2h = qo.nbytes
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(geo, ws),
+            "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "step": f"one wadg_app_solve_host call: H2D stage-0 state, {E2E_STEPS} time "
+                            f"steps, D2H Q (pinned host buffers, wall clock)",
+                    "calls": e2e_calls},
+            "gpu_launches": 15 * args.steps,
+            "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
+        sec, kind = time_cpu(geo, st0, dt, 2)
+        line["cpu_baseline"] = {"value": dofs * 10 / sec, "unit": UNIT,
+                                "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": kind,
+                                "sample": f"2 full LSRK-45 time steps (10 stages) of the whole "
+                                          f"workload (K={K}), OpenMP over elements"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    app.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def fp64_peak(stream):
+    import ctypes
+
+    from scratch_wadge_b200 import capi
+    L = capi.lib()
+    tf = ctypes.c_double()
+    ms = ctypes.c_float()
+    best = 0.0
+    for _ in range(3):
+        capi.check(L.wadg_probe_fp64_fma(ctypes.c_void_p(stream.cuda_stream), 20000,
+                                         ctypes.byref(tf), ctypes.byref(ms)), "fp64 probe")
+        best = max(best, tf.value)
+    return best
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-calls", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/*
+ * wadg.h — C ABI of the B200-native entropy-stable flux-differencing RHS.
+ *
+ * Drop-in for the OCCA kernel launches of the reference's host driver
+ * (`occaKernelRun(app->vol|surf|update, ...)`, euler.c:3610-3666).  Each
+ * kernel entry point keeps the argument list and meaning of the OKL kernel
+ * it replaces, with a leading context that carries what the reference passed
+ * as OCCA compile-time defines (euler.c:2879-2950: degree and sizes, gamma,
+ * tau) and the CUDA stream (the reference's `cmdx` stream, euler.c:2708-2710).
+ *
+ * Conventions (all entry points):
+ *   - pointers are DEVICE pointers owned by the caller; layouts are the
+ *     reference's (Q, rhsQ, resQ [K][Nfields][Nq]; Qf, rhsQf
+ *     [K][Nfields][Nfq*Nfaces]; vgeo [K][Nvgeo][Nq]; vfgeo
+ *     [K][Nvgeo][Nfq*Nfaces]; fgeo [K][Nfgeo][Nfq*Nfaces]; Jq [K][Nq];
+ *     operators column-major; mapPq [K][Nfq*Nfaces], field-strided);
+ *   - calls are asynchronous and ordered on the context's stream; nothing is
+ *     allocated per call;
+ *   - the return value is WADG_OK or an error code; wadg_last_error() gives a
+ *     message for the calling thread.  The reference aborts on errors
+ *     (ASD_ABORT); this library never aborts.
+ *   - FP64 throughout (the reference's dfloat=double build, types.h:33).
+ */
+#ifndef WADG_H
+#define WADG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum
+{
+  WADG_OK = 0,
+  WADG_ERR_INVALID = 1,     /* bad argument (null pointer, K < 0, ...) */
+  WADG_ERR_UNSUPPORTED = 2, /* (dim, N) not compiled, or sizes disagree */
+  WADG_ERR_CUDA = 3,        /* a CUDA call or kernel launch failed */
+  WADG_ERR_STATE = 4        /* non-physical state detected (check calls) */
+};
+
+typedef struct wadg_ctx wadg_ctx;
+
+typedef struct
+{
+  int dim;      /* 2 (triangles, 4 fields) or 3 (tetrahedra, 5 fields) */
+  int N;        /* polynomial degree; cubature degree M = 2N (euler.c:340) */
+  int Nq;       /* volume cubature points   (p_Nq)  */
+  int Nfq;      /* cubature points per face (p_Nfq) */
+  int Nfaces;   /* faces per element        (p_Nfaces) */
+  double gamma; /* p_gamma */
+  double tau;   /* p_TAU: Lax-Friedrichs penalty scale (3D; the 2D surface
+                   kernel of the reference hard-codes 1, Euler2D.okl:1423) */
+  void *stream; /* cudaStream_t the kernels run on; NULL = default stream */
+} wadg_params;
+
+/* Create / destroy a context.  Fails with WADG_ERR_UNSUPPORTED when (dim, N)
+ * is not compiled in or Nq/Nfq/Nfaces disagree with the compiled sizes. */
+int wadg_ctx_create(const wadg_params *p, wadg_ctx **out);
+int wadg_ctx_destroy(wadg_ctx *ctx);
+int wadg_ctx_set_stream(wadg_ctx *ctx, void *stream);
+const char *wadg_last_error(void);
+/* degrees compiled for `dim`, as a bit mask (bit N set = degree N) */
+int wadg_supported_degrees(int dim);
+
+/* ---------------------------------------------------------------- 3D kernels
+ * euler_vol_3d: Euler3Daffine.okl:152 (geometric factors constant per
+ * element, read at the first quadrature node).  rhsQ holds u(VqPq v) on entry
+ * and the volume flux-differencing term on exit; rhsQf receives the face-row
+ * block.  Drstq and Q are accepted and unused, as in the reference. */
+int wadg_euler_vol_3d(wadg_ctx *ctx, int K, const double *vgeo,
+                      const double *vfgeo, const double *nrJ,
+                      const double *nsJ, const double *ntJ, const double *Drq,
+                      const double *Dsq, const double *Dtq,
+                      const double *Drstq, const double *VqLq,
+                      const double *VfPq, const double *Q, const double *Qf,
+                      double *rhsQ, double *rhsQf);
+
+/* euler_vol_3d_curved: Euler3D.okl:2123 (pairwise averaged geometric
+ * factors from vgeo and vfgeo). Same arguments. */
+int wadg_euler_vol_3d_curved(wadg_ctx *ctx, int K, const double *vgeo,
+                             const double *vfgeo, const double *nrJ,
+                             const double *nsJ, const double *ntJ,
+                             const double *Drq, const double *Dsq,
+                             const double *Dtq, const double *Drstq,
+                             const double *VqLq, const double *VfPq,
+                             const double *Q, const double *Qf, double *rhsQ,
+                             double *rhsQf);
+
+/* euler_surf_3d: Euler3D.okl:3242 / Euler3Daffine.okl:421.  rhsQ += VqLq *
+ * (rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lambda-,lambda+) sJ (u+ - u-)).
+ * mapPq is the reference's uintloc_t array (declared int* in the OKL).
+ * rhsQf is read only (the affine OKL file also overwrites it with rho+ as a
+ * debug store that the next volume kernel discards; that store is not
+ * reproduced). */
+int wadg_euler_surf_3d(wadg_ctx *ctx, int K, const double *fgeo,
+                       const uint32_t *mapPq, const double *VqLq,
+                       const double *Qf, double *rhsQf, double *rhsQ);
+
+/* euler_update_3d: Euler3Daffine.okl:555 (affine M^-1 = -2 VqPq / J, LSRK
+ * stage, entropy projection).  euler_update_3d_curved: Euler3D.okl:2527
+ * (weight-adjusted M^-1 and weight-adjusted entropy projection). */
+int wadg_euler_update_3d(wadg_ctx *ctx, int K, const double *Jq,
+                         const double *VqPq, const double *VfPq, double fa,
+                         double fb, double fdt, double *rhsQ, double *resQ,
+                         double *Q, double *Qf);
+int wadg_euler_update_3d_curved(wadg_ctx *ctx, int K, const double *Jq,
+                                const double *VqPq, const double *VfPq,
+                                double fa, double fb, double fdt, double *rhsQ,
+                                double *resQ, double *Q, double *Qf);
+
+/* ---------------------------------------------------------------- 2D kernels
+ * euler_vol_2d: Euler2D.okl:235 (affine); euler_vol_2d_curved: :773. */
+int wadg_euler_vol_2d(wadg_ctx *ctx, int K, const double *vgeo,
+                      const double *vfgeo, const double *nrJ,
+                      const double *nsJ, const double *Drq, const double *Dsq,
+                      const double *VqLq, const double *VfPq, const double *Q,
+                      const double *Qf, double *rhsQ, double *rhsQf);
+int wadg_euler_vol_2d_curved(wadg_ctx *ctx, int K, const double *vgeo,
+                             const double *vfgeo, const double *nrJ,
+                             const double *nsJ, const double *Drq,
+                             const double *Dsq, const double *VqLq,
+                             const double *VfPq, const double *Q,
+                             const double *Qf, double *rhsQ, double *rhsQf);
+/* euler_surf_2d: Euler2D.okl:1357 */
+int wadg_euler_surf_2d(wadg_ctx *ctx, int K, const double *fgeo,
+                       const uint32_t *mapPq, const double *VqLq,
+                       const double *Qf, const double *rhsQf, double *rhsQ);
+/* euler_update_2d: Euler2D.okl:1498; euler_update_2d_curved: :1729 */
+int wadg_euler_update_2d(wadg_ctx *ctx, int K, const double *Jq,
+                         const double *VqPq, const double *VfPq, double fa,
+                         double fb, double fdt, double *rhsQ, double *resQ,
+                         double *Q, double *Qf);
+int wadg_euler_update_2d_curved(wadg_ctx *ctx, int K, const double *Jq,
+                                const double *VqPq, const double *VfPq,
+                                double fa, double fb, double fdt, double *rhsQ,
+                                double *resQ, double *Q, double *Qf);
+
+/* ------------------------------------------------------------ host driver
+ * The reference's app_t / rk_step / rk_run (euler.c:2607-2796, 3610-3738)
+ * over device buffers owned by the library.  Host arrays are copied once at
+ * creation (device_malloc, euler.c:2798-2877). */
+typedef struct wadg_app wadg_app;
+
+typedef struct
+{
+  /* geometry, per element (host pointers, reference layouts) */
+  const double *vgeo, *vfgeo, *fgeo, *Jq;
+  const uint32_t *mapPq;
+  /* reference-element operators (host pointers, column-major) */
+  const double *nrJ, *nsJ, *ntJ; /* ntJ ignored in 2D */
+  const double *Drq, *Dsq, *Dtq; /* Dtq ignored in 2D */
+  const double *VqLq, *VqPq, *VfPq;
+} wadg_host_data;
+
+/* curved = 0: affine kernels (vol/update without _curved); 1: curved/WADG */
+int wadg_app_create(const wadg_params *p, int K, int curved,
+                    const wadg_host_data *h, wadg_app **out);
+int wadg_app_destroy(wadg_app *app);
+/* Copy the solver state host -> device (any pointer may be NULL to skip). */
+int wadg_app_set_state(wadg_app *app, const double *Q, const double *rhsQ,
+                       const double *Qf, const double *resQ);
+/* Copy the solver state device -> host (any pointer may be NULL to skip);
+ * synchronises the app stream. */
+int wadg_app_get_state(wadg_app *app, double *Q, double *rhsQ, double *Qf,
+                       double *resQ);
+/* rk_step (euler.c:3610): vol, surf, update for one LSRK stage. */
+int wadg_rk_step(wadg_app *app, double rka, double rkb, double dt);
+/* rk_run (euler.c:3672): nsteps LSRK-45 time steps of size dt.  With
+ * use_graph != 0 one time step (15 launches) is captured once as a CUDA graph
+ * and replayed. Asynchronous. */
+int wadg_rk_run(wadg_app *app, double dt, int nsteps, int use_graph);
+/* The whole user-level solve with HOST buffers: copy the stage-0 state in,
+ * run nsteps, copy Q out (and the other state arrays if non-NULL).
+ * Synchronous. */
+int wadg_app_solve_host(wadg_app *app, const double *Q0, const double *rhsQ0,
+                        const double *Qf0, const double *resQ0, double dt,
+                        int nsteps, double *Q, double *rhsQ, double *Qf,
+                        double *resQ);
+int wadg_app_sync(wadg_app *app);
+/* device pointers of the state arrays (for zero-copy use and testing) */
+int wadg_app_state_ptrs(wadg_app *app, double **Q, double **rhsQ, double **Qf,
+                        double **resQ, double **rhsQf);
+/* Time `nsteps` time steps on the app stream with CUDA events (after the
+ * caller's warm-up); ms receives the elapsed device time. */
+int wadg_app_time_run(wadg_app *app, double dt, int nsteps, int use_graph,
+                      float *ms);
+/* Time each of the three kernels over `nstages` stages with CUDA events
+ * around every launch; ms[0..2] = total vol, surf, update time. */
+int wadg_app_time_kernels(wadg_app *app, double dt, int nstages, float *ms);
+
+/* ------------------------------------------------------------ measurement
+ * FP64 FMA throughput of the current GPU (the denominator of the volume
+ * kernel's FP64 roofline): a saturating FMA kernel timed with CUDA events on
+ * `stream`; tflops = 2 * FMAs / time.  No counterpart in the reference. */
+int wadg_probe_fp64_fma(void *stream, int iters, double *tflops, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,249 @@
+"""ctypes binding of the C ABI (include/wadg.h) and the host-side solver.
+
+The product path is the CUDA library libwadg_b200.so built in-tree by
+scratch_wadge_b200/build.py.  Loading fails loudly when it is missing: there is
+no CPU fallback.
+
+* ``Context``   kernel-level entry points with the OKL argument lists
+                (device pointers as ints, e.g. torch ``tensor.data_ptr()``).
+* ``App``       the reference's app_t / rk_step / rk_run over library-owned
+                device buffers (euler.c:2607-2796, 3610-3738).
+* ``Solver``    mesh + operators + geometry + stage-0 state + App, the
+                user-level object (the reference's main(), euler.c:3833-4350).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import ic as IC
+from . import mesh as M
+from . import refops as R
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwadg_b200.so")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_U32 = ctypes.POINTER(ctypes.c_uint32)
+_V = ctypes.c_void_p
+_lib = None
+
+
+class WadgError(RuntimeError):
+    pass
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("N", ctypes.c_int), ("Nq", ctypes.c_int),
+                ("Nfq", ctypes.c_int), ("Nfaces", ctypes.c_int), ("gamma", ctypes.c_double),
+                ("tau", ctypes.c_double), ("stream", ctypes.c_void_p)]
+
+
+class HostData(ctypes.Structure):
+    _fields_ = [(n, _D) for n in ("vgeo", "vfgeo", "fgeo", "Jq")] + [("mapPq", _U32)] + \
+               [(n, _D) for n in ("nrJ", "nsJ", "ntJ", "Drq", "Dsq", "Dtq", "VqLq", "VqPq", "VfPq")]
+
+
+def lib():
+    """The CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise WadgError(f"{LIB_PATH} missing: run scratch_wadge_b200/build.py (no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.wadg_last_error.restype = ctypes.c_char_p
+        i, d, v = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+        for name in ("wadg_euler_vol_3d", "wadg_euler_vol_3d_curved"):
+            getattr(L, name).argtypes = [v, i] + [v] * 15
+        for name in ("wadg_euler_vol_2d", "wadg_euler_vol_2d_curved"):
+            getattr(L, name).argtypes = [v, i] + [v] * 12
+        for name in ("wadg_euler_surf_3d", "wadg_euler_surf_2d"):
+            getattr(L, name).argtypes = [v, i] + [v] * 6
+        for name in ("wadg_euler_update_3d", "wadg_euler_update_3d_curved",
+                     "wadg_euler_update_2d", "wadg_euler_update_2d_curved"):
+            getattr(L, name).argtypes = [v, i, v, v, v, d, d, d, v, v, v, v]
+        L.wadg_rk_step.argtypes = [v, d, d, d]
+        L.wadg_rk_run.argtypes = [v, d, i, i]
+        L.wadg_app_time_run.argtypes = [v, d, i, i, ctypes.POINTER(ctypes.c_float)]
+        L.wadg_app_time_kernels.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
+        L.wadg_app_solve_host.argtypes = [v, v, v, v, v, d, i, v, v, v, v]
+        L.wadg_app_set_state.argtypes = [v, v, v, v, v]
+        L.wadg_app_get_state.argtypes = [v, v, v, v, v]
+        L.wadg_app_state_ptrs.argtypes = [v] + [ctypes.POINTER(ctypes.c_void_p)] * 5
+        L.wadg_app_create.argtypes = [ctypes.POINTER(Params), i, i, ctypes.POINTER(HostData),
+                                      ctypes.POINTER(ctypes.c_void_p)]
+        L.wadg_ctx_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]
+        L.wadg_ctx_destroy.argtypes = [v]
+        L.wadg_app_destroy.argtypes = [v]
+        L.wadg_app_sync.argtypes = [v]
+        L.wadg_ctx_set_stream.argtypes = [v, v]
+        _lib = L
+    return _lib
+
+
+def check(code: int, what: str = ""):
+    if code != 0:
+        msg = lib().wadg_last_error().decode()
+        raise WadgError(f"{what} failed ({code}): {msg}")
+
+
+def params_for(ops: R.RefOps, gamma=1.4, tau=1.0, stream=None) -> Params:
+    return Params(ops.dim, ops.N, ops.Nq, ops.Nfq, ops.Nfaces, gamma, tau, stream)
+
+
+class Context:
+    """Kernel-level API: each method is one OKL kernel launch on device
+    pointers (ints)."""
+
+    def __init__(self, ops: R.RefOps, gamma=1.4, tau=1.0, stream=None):
+        self.ops = ops
+        self.p = params_for(ops, gamma, tau, stream)
+        h = ctypes.c_void_p()
+        check(lib().wadg_ctx_create(ctypes.byref(self.p), ctypes.byref(h)), "wadg_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().wadg_ctx_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_stream(self, stream):
+        check(lib().wadg_ctx_set_stream(self.h, stream), "set_stream")
+
+    def vol(self, curved, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf):
+        L = lib()
+        if self.ops.dim == 3:
+            fn = L.wadg_euler_vol_3d_curved if curved else L.wadg_euler_vol_3d
+            check(fn(self.h, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, None, VqLq, VfPq, None,
+                     Qf, rhsQ, rhsQf), "vol")
+        else:
+            fn = L.wadg_euler_vol_2d_curved if curved else L.wadg_euler_vol_2d
+            check(fn(self.h, K, vgeo, vfgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, None, Qf, rhsQ, rhsQf), "vol")
+
+    def surf(self, K, fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ):
+        L = lib()
+        fn = L.wadg_euler_surf_3d if self.ops.dim == 3 else L.wadg_euler_surf_2d
+        check(fn(self.h, K, fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ), "surf")
+
+    def update(self, curved, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf):
+        L = lib()
+        d = self.ops.dim
+        fn = getattr(L, f"wadg_euler_update_{d}d" + ("_curved" if curved else ""))
+        check(fn(self.h, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf), "update")
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+class App:
+    """Library-owned device state and the LSRK driver."""
+
+    def __init__(self, geo: M.Geometry, curved: bool, gamma=1.4, tau=1.0, stream=None):
+        ops = geo.ops
+        self.geo, self.ops, self.curved = geo, ops, bool(curved)
+        self.K = geo.K
+        self.p = params_for(ops, gamma, tau, stream)
+        c = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        self._keep = dict(
+            vgeo=c(geo.vgeo), vfgeo=c(geo.vfgeo), fgeo=c(geo.fgeo), Jq=c(geo.Jq),
+            mapPq=np.ascontiguousarray(geo.mapPq, dtype=np.uint32),
+            nrJ=c(ops.nrJ), nsJ=c(ops.nsJ), ntJ=c(ops.ntJ), Drq=c(ops.fortran("Drq")),
+            Dsq=c(ops.fortran("Dsq")), Dtq=c(ops.fortran("Dtq")), VqLq=c(ops.fortran("VqLq")),
+            VqPq=c(ops.fortran("VqPq")), VfPq=c(ops.fortran("VfPq")))
+        k = self._keep
+        hd = HostData(*([_dp(k[n]) for n in ("vgeo", "vfgeo", "fgeo", "Jq")] +
+                        [k["mapPq"].ctypes.data_as(_U32)] +
+                        [_dp(k[n]) for n in ("nrJ", "nsJ", "ntJ", "Drq", "Dsq", "Dtq", "VqLq", "VqPq", "VfPq")]))
+        h = ctypes.c_void_p()
+        check(lib().wadg_app_create(ctypes.byref(self.p), self.K, int(self.curved), ctypes.byref(hd),
+                                    ctypes.byref(h)), "wadg_app_create")
+        self.h = h
+        Nf, Nq, NfqNf = ops.Nfields, ops.Nq, ops.NfqNf
+        self.vshape, self.fshape = (self.K, Nf, Nq), (self.K, Nf, NfqNf)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wadg_app_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_state(self, Q=None, rhsQ=None, Qf=None, resQ=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (Q, rhsQ, Qf, resQ)]
+        check(lib().wadg_app_set_state(self.h, *[None if a is None else a.ctypes.data for a in arrs]), "set_state")
+        check(lib().wadg_app_sync(self.h), "sync")
+
+    def get_state(self):
+        Q, rhsQ, resQ = (np.empty(self.vshape) for _ in range(3))
+        Qf = np.empty(self.fshape)
+        check(lib().wadg_app_get_state(self.h, Q.ctypes.data, rhsQ.ctypes.data, Qf.ctypes.data,
+                                       resQ.ctypes.data), "get_state")
+        return dict(Q=Q, rhsQ=rhsQ, Qf=Qf, resQ=resQ)
+
+    def state_ptrs(self):
+        ps = [ctypes.c_void_p() for _ in range(5)]
+        check(lib().wadg_app_state_ptrs(self.h, *[ctypes.byref(p) for p in ps]), "state_ptrs")
+        return dict(zip(("Q", "rhsQ", "Qf", "resQ", "rhsQf"), [p.value for p in ps]))
+
+    def rk_step(self, rka, rkb, dt):
+        check(lib().wadg_rk_step(self.h, rka, rkb, dt), "rk_step")
+
+    def rk_run(self, dt, nsteps, graph=True):
+        check(lib().wadg_rk_run(self.h, dt, nsteps, int(graph)), "rk_run")
+
+    def sync(self):
+        check(lib().wadg_app_sync(self.h), "sync")
+
+    def solve_host(self, Q0, rhsQ0, Qf0, dt, nsteps, resQ0=None, out=None):
+        """User-level solve with host buffers (H2D, nsteps, D2H of Q)."""
+        Q = out if out is not None else np.empty(self.vshape)
+        c = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).ctypes.data
+        check(lib().wadg_app_solve_host(self.h, c(Q0), c(rhsQ0), c(Qf0), c(resQ0), dt, nsteps,
+                                        Q.ctypes.data, None, None, None), "solve_host")
+        return Q
+
+    def time_run(self, dt, nsteps, graph=True):
+        ms = ctypes.c_float()
+        check(lib().wadg_app_time_run(self.h, dt, nsteps, int(graph), ctypes.byref(ms)), "time_run")
+        return ms.value
+
+    def time_kernels(self, dt, nstages):
+        ms = (ctypes.c_float * 3)()
+        check(lib().wadg_app_time_kernels(self.h, dt, nstages, ms), "time_kernels")
+        return list(ms)
+
+
+class Solver:
+    """Mesh, operators, geometry, stage-0 state and the device driver: what
+    the reference's main() sets up before rk_run (euler.c:3833-4215)."""
+
+    def __init__(self, mesh: M.Mesh, N: int, curved: bool, ic="taylor_green", gamma=1.4, tau=1.0,
+                 ic_args=None, stream=None):
+        self.mesh, self.N, self.curved, self.gamma = mesh, N, curved, gamma
+        self.geo = M.build_geometry(mesh, N)
+        self.ic, self.ic_args = ic, dict(ic_args or {})
+        U0 = IC.initial_state(self.geo, ic, gamma, **self.ic_args)
+        self.Q0, self.rhsQ0, self.Qf0, self.resQ0 = IC.stage0(self.geo, U0, gamma)
+        self.app = App(self.geo, curved, gamma, tau, stream)
+        self.reset()
+
+    @property
+    def ops(self):
+        return self.geo.ops
+
+    @property
+    def dofs(self):
+        """DOF per field = K * Np (the throughput unit)."""
+        return self.geo.K * self.ops.Np
+
+    def reset(self):
+        self.app.set_state(self.Q0, self.rhsQ0, self.Qf0, self.resQ0)
+
+    def time_step(self, CFL, FinalTime=None, nsteps=None):
+        return IC.time_step(self.geo, CFL, self.N, FinalTime, nsteps)

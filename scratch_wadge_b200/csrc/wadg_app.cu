@@ -1,0 +1,410 @@
+// Host driver: the reference's app_t / rk_step / rk_run (euler.c:2607-2796,
+// 3610-3738) on device buffers owned by the library, with one LSRK-45 time
+// step (5 stages x 3 kernels) captured as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/wadg.h"
+
+namespace wadg_internal {
+void set_error(const std::string &msg);  // wadg_capi.cu
+}
+
+namespace {
+// LSRK-45 (Carpenter & Kennedy) coefficients, euler.c:2779-2796
+const double RK4A[5] = {0.0, -567301805773.0 / 1357537059087.0,
+                        -2404267990393.0 / 2016746695238.0,
+                        -3550918686646.0 / 2091501179385.0,
+                        -1275806237668.0 / 842570457699.0};
+const double RK4B[5] = {1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                        1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                        2277821191437.0 / 14882151754819.0};
+
+int afail(int code, const char *msg, cudaError_t e = cudaSuccess) {
+  std::string m = msg;
+  if (e != cudaSuccess) {
+    m += ": ";
+    m += cudaGetErrorString(e);
+  }
+  wadg_internal::set_error(m);
+  return code;
+}
+}  // namespace
+
+struct wadg_app {
+  wadg_ctx *ctx = nullptr;
+  wadg_params p{};
+  int K = 0, curved = 0;
+  int Nq = 0, NfqNf = 0, Nf = 0, Nvgeo = 0, Nfgeo = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // geometry and operators
+  double *vgeo = nullptr, *vfgeo = nullptr, *fgeo = nullptr, *Jq = nullptr;
+  uint32_t *mapPq = nullptr;
+  double *nrJ = nullptr, *nsJ = nullptr, *ntJ = nullptr, *Drq = nullptr, *Dsq = nullptr,
+         *Dtq = nullptr, *Drstq = nullptr, *VqLq = nullptr, *VqPq = nullptr, *VfPq = nullptr;
+  // solver state
+  double *Q = nullptr, *rhsQ = nullptr, *Qf = nullptr, *resQ = nullptr, *rhsQf = nullptr;
+  // graph of one time step
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = 0.0;
+};
+
+namespace {
+
+template <class T>
+int upload(T **dst, const T *src, size_t n, cudaStream_t s) {
+  cudaError_t e = cudaMalloc((void **)dst, sizeof(T) * (n ? n : 1));
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaMalloc", e);
+  if (src) {
+    e = cudaMemcpyAsync(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaMemcpyAsync", e);
+  } else {
+    e = cudaMemsetAsync(*dst, 0, sizeof(T) * (n ? n : 1), s);
+    if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaMemsetAsync", e);
+  }
+  return WADG_OK;
+}
+
+void free_all(wadg_app *a) {
+  double *bufs[] = {a->vgeo, a->vfgeo, a->fgeo, a->Jq, a->nrJ, a->nsJ, a->ntJ, a->Drq, a->Dsq,
+                    a->Dtq, a->Drstq, a->VqLq, a->VqPq, a->VfPq, a->Q, a->rhsQ, a->Qf, a->resQ,
+                    a->rhsQf};
+  for (double *b : bufs)
+    if (b) cudaFree(b);
+  if (a->mapPq) cudaFree(a->mapPq);
+  if (a->graph) cudaGraphExecDestroy(a->graph);
+  if (a->ctx) wadg_ctx_destroy(a->ctx);
+  if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
+}
+
+int stage(wadg_app *a, double rka, double rkb, double dt) {
+  int r;
+  const int K = a->K;
+  if (a->p.dim == 3) {
+    r = a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
+                                             a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq,
+                                             a->Q, a->Qf, a->rhsQ, a->rhsQf)
+                  : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ, a->Drq,
+                                      a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q, a->Qf,
+                                      a->rhsQ, a->rhsQf);
+    if (r) return r;
+    r = wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf, a->rhsQf, a->rhsQ);
+    if (r) return r;
+    r = a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+                                                a->rhsQ, a->resQ, a->Q, a->Qf)
+                  : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, a->rhsQ,
+                                         a->resQ, a->Q, a->Qf);
+  } else {
+    r = a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
+                                             a->Dsq, a->VqLq, a->VfPq, a->Q, a->Qf, a->rhsQ,
+                                             a->rhsQf)
+                  : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq, a->Dsq,
+                                      a->VqLq, a->VfPq, a->Q, a->Qf, a->rhsQ, a->rhsQf);
+    if (r) return r;
+    r = wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf, a->rhsQf, a->rhsQ);
+    if (r) return r;
+    r = a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+                                                a->rhsQ, a->resQ, a->Q, a->Qf)
+                  : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, a->rhsQ,
+                                         a->resQ, a->Q, a->Qf);
+  }
+  return r;
+}
+
+int capture_step(wadg_app *a, double dt) {
+  if (a->graph && a->graph_dt == dt) return WADG_OK;
+  if (a->graph) {
+    cudaGraphExecDestroy(a->graph);
+    a->graph = nullptr;
+  }
+  cudaGraph_t g;
+  cudaError_t e = cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaStreamBeginCapture", e);
+  int r = WADG_OK;
+  for (int s = 0; s < 5 && r == WADG_OK; ++s) r = stage(a, RK4A[s], RK4B[s], dt);
+  e = cudaStreamEndCapture(a->stream, &g);
+  if (r) return r;
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaStreamEndCapture", e);
+  e = cudaGraphInstantiate(&a->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaGraphInstantiate", e);
+  a->graph_dt = dt;
+  return WADG_OK;
+}
+
+bool valid_map(const uint32_t *m, int K, int NfqNf, int Nf) {
+  const size_t per = (size_t)NfqNf * Nf;
+  for (size_t i = 0; i < (size_t)K * NfqNf; ++i) {
+    const size_t e = m[i] / per, j = m[i] % per;
+    if (e >= (size_t)K || j >= (size_t)NfqNf) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wadg_app_create(const wadg_params *p, int K, int curved, const wadg_host_data *h,
+                    wadg_app **out) {
+  if (!p || !h || !out || K <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  *out = nullptr;
+  wadg_app *a = new wadg_app;
+  a->p = *p;
+  a->K = K;
+  a->curved = curved ? 1 : 0;
+  a->Nq = p->Nq;
+  a->NfqNf = p->Nfq * p->Nfaces;
+  a->Nf = p->dim + 2;
+  a->Nvgeo = p->dim * p->dim;
+  a->Nfgeo = p->dim + 1;
+  if (p->stream) {
+    a->stream = (cudaStream_t)p->stream;
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete a;
+      return afail(WADG_ERR_CUDA, "cudaStreamCreate", e);
+    }
+    a->own_stream = true;
+  }
+  wadg_params cp = *p;
+  cp.stream = a->stream;
+  int r = wadg_ctx_create(&cp, &a->ctx);
+  if (r) {
+    free_all(a);
+    delete a;
+    return r;
+  }
+  const bool d3 = p->dim == 3;
+  if (!h->vgeo || !h->fgeo || !h->Jq || !h->mapPq || !h->nrJ || !h->nsJ || !h->Drq || !h->Dsq ||
+      !h->VqLq || !h->VqPq || !h->VfPq || (curved && !h->vfgeo) || (d3 && (!h->ntJ || !h->Dtq))) {
+    free_all(a);
+    delete a;
+    return afail(WADG_ERR_INVALID, "missing host array");
+  }
+  if (!valid_map(h->mapPq, K, a->NfqNf, a->Nf)) {
+    free_all(a);
+    delete a;
+    return afail(WADG_ERR_INVALID, "mapPq holds an index outside [0, K*NfqNf*Nfields)");
+  }
+  const size_t Nq = a->Nq, NfqNf = a->NfqNf, Nf = a->Nf;
+  cudaStream_t s = a->stream;
+  if ((r = upload(&a->vgeo, h->vgeo, K * Nq * a->Nvgeo, s)) ||
+      (r = upload(&a->vfgeo, h->vfgeo, h->vfgeo ? K * NfqNf * a->Nvgeo : 1, s)) ||
+      (r = upload(&a->fgeo, h->fgeo, K * NfqNf * a->Nfgeo, s)) ||
+      (r = upload(&a->Jq, h->Jq, K * Nq, s)) ||
+      (r = upload(&a->mapPq, h->mapPq, K * NfqNf, s)) ||
+      (r = upload(&a->nrJ, h->nrJ, NfqNf, s)) || (r = upload(&a->nsJ, h->nsJ, NfqNf, s)) ||
+      (r = upload(&a->ntJ, d3 ? h->ntJ : nullptr, NfqNf, s)) ||
+      (r = upload(&a->Drq, h->Drq, Nq * Nq, s)) || (r = upload(&a->Dsq, h->Dsq, Nq * Nq, s)) ||
+      (r = upload(&a->Dtq, d3 ? h->Dtq : nullptr, Nq * Nq, s)) ||
+      (r = upload(&a->Drstq, (const double *)nullptr, 3 * Nq * Nq, s)) ||
+      (r = upload(&a->VqLq, h->VqLq, Nq * NfqNf, s)) ||
+      (r = upload(&a->VqPq, h->VqPq, Nq * Nq, s)) ||
+      (r = upload(&a->VfPq, h->VfPq, NfqNf * Nq, s)) ||
+      (r = upload(&a->Q, (const double *)nullptr, K * Nq * Nf, s)) ||
+      (r = upload(&a->rhsQ, (const double *)nullptr, K * Nq * Nf, s)) ||
+      (r = upload(&a->resQ, (const double *)nullptr, K * Nq * Nf, s)) ||
+      (r = upload(&a->Qf, (const double *)nullptr, K * NfqNf * Nf, s)) ||
+      (r = upload(&a->rhsQf, (const double *)nullptr, K * NfqNf * Nf, s))) {
+    free_all(a);
+    delete a;
+    return r;
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    free_all(a);
+    delete a;
+    return afail(WADG_ERR_CUDA, "upload", e);
+  }
+  *out = a;
+  return WADG_OK;
+}
+
+int wadg_app_destroy(wadg_app *a) {
+  if (!a) return WADG_OK;
+  cudaStreamSynchronize(a->stream);
+  free_all(a);
+  delete a;
+  return WADG_OK;
+}
+
+int wadg_app_set_state(wadg_app *a, const double *Q, const double *rhsQ, const double *Qf,
+                       const double *resQ) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  const size_t nv = (size_t)a->K * a->Nq * a->Nf * sizeof(double);
+  const size_t nf = (size_t)a->K * a->NfqNf * a->Nf * sizeof(double);
+  struct {
+    double *d;
+    const double *h;
+    size_t n;
+  } c[] = {{a->Q, Q, nv}, {a->rhsQ, rhsQ, nv}, {a->Qf, Qf, nf}, {a->resQ, resQ, nv}};
+  for (auto &x : c)
+    if (x.h) {
+      cudaError_t e = cudaMemcpyAsync(x.d, x.h, x.n, cudaMemcpyHostToDevice, a->stream);
+      if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "set_state", e);
+    }
+  return WADG_OK;
+}
+
+int wadg_app_get_state(wadg_app *a, double *Q, double *rhsQ, double *Qf, double *resQ) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  const size_t nv = (size_t)a->K * a->Nq * a->Nf * sizeof(double);
+  const size_t nf = (size_t)a->K * a->NfqNf * a->Nf * sizeof(double);
+  struct {
+    double *h;
+    const double *d;
+    size_t n;
+  } c[] = {{Q, a->Q, nv}, {rhsQ, a->rhsQ, nv}, {Qf, a->Qf, nf}, {resQ, a->resQ, nv}};
+  for (auto &x : c)
+    if (x.h) {
+      cudaError_t e = cudaMemcpyAsync(x.h, x.d, x.n, cudaMemcpyDeviceToHost, a->stream);
+      if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "get_state", e);
+    }
+  cudaError_t e = cudaStreamSynchronize(a->stream);
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "get_state sync", e);
+  return WADG_OK;
+}
+
+int wadg_rk_step(wadg_app *a, double rka, double rkb, double dt) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  return stage(a, rka, rkb, dt);
+}
+
+int wadg_rk_run(wadg_app *a, double dt, int nsteps, int use_graph) {
+  if (!a || nsteps < 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  if (use_graph) {
+    int r = capture_step(a, dt);
+    if (r) return r;
+    for (int t = 0; t < nsteps; ++t) {
+      cudaError_t e = cudaGraphLaunch(a->graph, a->stream);
+      if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaGraphLaunch", e);
+    }
+    return WADG_OK;
+  }
+  for (int t = 0; t < nsteps; ++t)
+    for (int s = 0; s < 5; ++s) {
+      int r = stage(a, RK4A[s], RK4B[s], dt);
+      if (r) return r;
+    }
+  return WADG_OK;
+}
+
+int wadg_app_solve_host(wadg_app *a, const double *Q0, const double *rhsQ0, const double *Qf0,
+                        const double *resQ0, double dt, int nsteps, double *Q, double *rhsQ,
+                        double *Qf, double *resQ) {
+  if (!a || !Q0 || !rhsQ0 || !Qf0 || !Q) return afail(WADG_ERR_INVALID, "invalid argument");
+  int r = wadg_app_set_state(a, Q0, rhsQ0, Qf0, resQ0);
+  if (r) return r;
+  if (!resQ0) {
+    cudaError_t e = cudaMemsetAsync(a->resQ, 0, (size_t)a->K * a->Nq * a->Nf * sizeof(double),
+                                    a->stream);
+    if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "memset resQ", e);
+  }
+  if ((r = wadg_rk_run(a, dt, nsteps, 1))) return r;
+  return wadg_app_get_state(a, Q, rhsQ, Qf, resQ);
+}
+
+int wadg_app_sync(wadg_app *a) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  cudaError_t e = cudaStreamSynchronize(a->stream);
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "sync", e);
+  return WADG_OK;
+}
+
+int wadg_app_state_ptrs(wadg_app *a, double **Q, double **rhsQ, double **Qf, double **resQ,
+                        double **rhsQf) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  if (Q) *Q = a->Q;
+  if (rhsQ) *rhsQ = a->rhsQ;
+  if (Qf) *Qf = a->Qf;
+  if (resQ) *resQ = a->resQ;
+  if (rhsQf) *rhsQf = a->rhsQf;
+  return WADG_OK;
+}
+
+int wadg_app_time_run(wadg_app *a, double dt, int nsteps, int use_graph, float *ms) {
+  if (!a || !ms) return afail(WADG_ERR_INVALID, "invalid argument");
+  if (use_graph) {
+    int r = capture_step(a, dt);
+    if (r) return r;
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, a->stream);
+  int r = wadg_rk_run(a, dt, nsteps, use_graph);
+  cudaEventRecord(e1, a->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  if (!r && e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "time_run", e);
+  return WADG_OK;
+}
+
+int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
+  if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  const int K = a->K;
+  cudaEvent_t ev[4];
+  for (auto &x : ev) cudaEventCreate(&x);
+  float tot[3] = {0, 0, 0};
+  int r = WADG_OK;
+  for (int s = 0; s < nstages && r == WADG_OK; ++s) {
+    const double rka = RK4A[s % 5], rkb = RK4B[s % 5];
+    cudaEventRecord(ev[0], a->stream);
+    if (a->p.dim == 3)
+      r = a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
+                                               a->ntJ, a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq,
+                                               a->VfPq, a->Q, a->Qf, a->rhsQ, a->rhsQf)
+                    : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
+                                        a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q,
+                                        a->Qf, a->rhsQ, a->rhsQf);
+    else
+      r = a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
+                                               a->Drq, a->Dsq, a->VqLq, a->VfPq, a->Q, a->Qf,
+                                               a->rhsQ, a->rhsQf)
+                    : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
+                                        a->Dsq, a->VqLq, a->VfPq, a->Q, a->Qf, a->rhsQ, a->rhsQf);
+    cudaEventRecord(ev[1], a->stream);
+    if (!r)
+      r = a->p.dim == 3 ? wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf,
+                                             a->rhsQf, a->rhsQ)
+                        : wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf,
+                                             a->rhsQf, a->rhsQ);
+    cudaEventRecord(ev[2], a->stream);
+    if (!r) {
+      if (a->p.dim == 3)
+        r = a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
+                                                    dt, a->rhsQ, a->resQ, a->Q, a->Qf)
+                      : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+                                             a->rhsQ, a->resQ, a->Q, a->Qf);
+      else
+        r = a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
+                                                    dt, a->rhsQ, a->resQ, a->Q, a->Qf)
+                      : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+                                             a->rhsQ, a->resQ, a->Q, a->Qf);
+    }
+    cudaEventRecord(ev[3], a->stream);
+    cudaError_t e = cudaEventSynchronize(ev[3]);
+    if (e != cudaSuccess && !r) r = afail(WADG_ERR_CUDA, "time_kernels", e);
+    if (!r)
+      for (int q = 0; q < 3; ++q) {
+        float t;
+        cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+        tot[q] += t;
+      }
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (r) return r;
+  for (int q = 0; q < 3; ++q) ms[q] = tot[q];
+  return WADG_OK;
+}
+
+}  // extern "C"

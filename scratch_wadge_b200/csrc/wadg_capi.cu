@@ -1,0 +1,317 @@
+// C ABI of the library: context, kernel entry points (one per OKL kernel of the
+// reference), and the host driver (app / rk_step / rk_run).  See include/wadg.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/wadg.h"
+#include "wadg_kernels.cuh"
+
+using namespace wadg;
+
+struct wadg_ctx {
+  int dim, N, Nq, Nfq, Nfaces;
+  Phys phys;
+  cudaStream_t stream;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) return fail(WADG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return WADG_OK;
+}
+
+int after_launch(const char *name) { return cuda_check(cudaGetLastError(), name); }
+
+constexpr int pickE(int target, int per) { return per >= target ? 1 : target / per; }
+
+template <int DIM, int N> constexpr int volE() { return pickE(320, Elem<DIM, N>::NN); }
+template <int DIM, int N> constexpr int surfE() {
+  return pickE(256, Elem<DIM, N>::NfqNf > Elem<DIM, N>::Nq ? Elem<DIM, N>::NfqNf : Elem<DIM, N>::Nq);
+}
+template <int DIM, int N> constexpr int updE() { return pickE(256, Elem<DIM, N>::Nq); }
+
+template <int DIM, int N, bool CURVED>
+int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+               const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+               const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
+               const double *Qf, double *rhsQ, double *rhsQf) {
+  constexpr int E = volE<DIM, N>();
+  using C = VolCfg<DIM, N, CURVED, E>;
+  auto kern = vol_kernel<DIM, N, CURVED, E>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    attr = true;
+  }
+  const int grid = (K + E - 1) / E;
+  kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
+                                                   VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
+  return after_launch("vol kernel");
+}
+
+template <int DIM, int N>
+int launch_surf(const wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
+                const double *VqLq, const double *Qf, const double *rhsQf, double *rhsQ) {
+  constexpr int E = surfE<DIM, N>();
+  using C = SurfCfg<DIM, N, E>;
+  const int grid = (K + E - 1) / E;
+  surf_kernel<DIM, N, E><<<grid, C::threads, C::smem, c->stream>>>(K, fgeo, mapPq, VqLq, Qf,
+                                                                    rhsQf, rhsQ, c->phys);
+  return after_launch("surf kernel");
+}
+
+template <int DIM, int N, bool CURVED>
+int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq,
+                  const double *VfPq, double fa, double fb, double fdt, double *rhsQ,
+                  double *resQ, double *Q, double *Qf) {
+  constexpr int E = updE<DIM, N>();
+  using C = UpdCfg<DIM, N, CURVED, E>;
+  const int grid = (K + E - 1) / E;
+  update_kernel<DIM, N, CURVED, E><<<grid, C::threads, C::smem, c->stream>>>(
+      K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf, c->phys);
+  return after_launch("update kernel");
+}
+
+// (dim, N) -> template instantiation
+#define WADG_DISPATCH(c, CALL)                                 \
+  do {                                                         \
+    if ((c)->dim == 2) {                                       \
+      switch ((c)->N) {                                        \
+        case 1: { constexpr int D_ = 2, N_ = 1; CALL; }        \
+        case 2: { constexpr int D_ = 2, N_ = 2; CALL; }        \
+        case 3: { constexpr int D_ = 2, N_ = 3; CALL; }        \
+        case 4: { constexpr int D_ = 2, N_ = 4; CALL; }        \
+      }                                                        \
+    } else {                                                   \
+      switch ((c)->N) {                                        \
+        case 1: { constexpr int D_ = 3, N_ = 1; CALL; }        \
+        case 2: { constexpr int D_ = 3, N_ = 2; CALL; }        \
+        case 3: { constexpr int D_ = 3, N_ = 3; CALL; }        \
+        case 4: { constexpr int D_ = 3, N_ = 4; CALL; }        \
+      }                                                        \
+    }                                                          \
+    return fail(WADG_ERR_UNSUPPORTED, "degree not compiled");  \
+  } while (0)
+
+int check_ctx(const wadg_ctx *c, int dim, int K) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  if (c->dim != dim) return fail(WADG_ERR_INVALID, "context is %dD, kernel is %dD", c->dim, dim);
+  if (K < 0) return fail(WADG_ERR_INVALID, "K < 0");
+  return WADG_OK;
+}
+
+bool any_null(std::initializer_list<const void *> ps) {
+  for (auto p : ps)
+    if (!p) return true;
+  return false;
+}
+
+template <int DIM, int N> bool sizes_match(const wadg_params *p) {
+  using El = Elem<DIM, N>;
+  return p->Nq == El::Nq && p->Nfq == El::Nfq && p->Nfaces == El::Nfaces;
+}
+
+}  // namespace
+
+namespace wadg_internal {
+void set_error(const std::string &msg) { g_err = msg; }
+}  // namespace wadg_internal
+
+extern "C" {
+
+const char *wadg_last_error(void) { return g_err.c_str(); }
+
+int wadg_supported_degrees(int dim) { return (dim == 2 || dim == 3) ? 0x1e : 0; }
+
+int wadg_ctx_create(const wadg_params *p, wadg_ctx **out) {
+  if (!p || !out) return fail(WADG_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (p->dim != 2 && p->dim != 3) return fail(WADG_ERR_INVALID, "dim must be 2 or 3");
+  bool ok = false;
+  if (p->dim == 2) {
+    switch (p->N) {
+      case 1: ok = sizes_match<2, 1>(p); break;
+      case 2: ok = sizes_match<2, 2>(p); break;
+      case 3: ok = sizes_match<2, 3>(p); break;
+      case 4: ok = sizes_match<2, 4>(p); break;
+      default: return fail(WADG_ERR_UNSUPPORTED, "2D degree %d not compiled", p->N);
+    }
+  } else {
+    switch (p->N) {
+      case 1: ok = sizes_match<3, 1>(p); break;
+      case 2: ok = sizes_match<3, 2>(p); break;
+      case 3: ok = sizes_match<3, 3>(p); break;
+      case 4: ok = sizes_match<3, 4>(p); break;
+      default: return fail(WADG_ERR_UNSUPPORTED, "3D degree %d not compiled", p->N);
+    }
+  }
+  if (!ok)
+    return fail(WADG_ERR_UNSUPPORTED, "sizes Nq=%d Nfq=%d Nfaces=%d do not match degree %d", p->Nq,
+                p->Nfq, p->Nfaces, p->N);
+  if (!(p->gamma > 1.0)) return fail(WADG_ERR_INVALID, "gamma must be > 1");
+  wadg_ctx *c = new wadg_ctx;
+  c->dim = p->dim;
+  c->N = p->N;
+  c->Nq = p->Nq;
+  c->Nfq = p->Nfq;
+  c->Nfaces = p->Nfaces;
+  c->phys.gamma = p->gamma;
+  c->phys.gm1 = p->gamma - 1.0;
+  c->phys.cbeta = 1.0 / (2.0 * (p->gamma - 1.0));
+  c->phys.tau = p->tau;
+  c->stream = (cudaStream_t)p->stream;
+  *out = c;
+  return WADG_OK;
+}
+
+int wadg_ctx_destroy(wadg_ctx *ctx) {
+  delete ctx;
+  return WADG_OK;
+}
+
+int wadg_ctx_set_stream(wadg_ctx *ctx, void *stream) {
+  if (!ctx) return fail(WADG_ERR_INVALID, "null context");
+  ctx->stream = (cudaStream_t)stream;
+  return WADG_OK;
+}
+
+// ------------------------------------------------------------------ 3D
+int wadg_euler_vol_3d(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                      const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+                      const double *Dsq, const double *Dtq, const double *Drstq,
+                      const double *VqLq, const double *VfPq, const double *Q, const double *Qf,
+                      double *rhsQ, double *rhsQf) {
+  (void)Drstq; (void)Q; (void)vfgeo;
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_vol<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
+                                                      Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
+}
+
+int wadg_euler_vol_3d_curved(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                             const double *nrJ, const double *nsJ, const double *ntJ,
+                             const double *Drq, const double *Dsq, const double *Dtq,
+                             const double *Drstq, const double *VqLq, const double *VfPq,
+                             const double *Q, const double *Qf, double *rhsQ, double *rhsQf) {
+  (void)Drstq; (void)Q;
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_vol<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
+                                                     Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
+}
+
+int wadg_euler_surf_3d(wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
+                       const double *VqLq, const double *Qf, double *rhsQf, double *rhsQ) {
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_surf<D_, N_>(c, K, fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ)));
+}
+
+int wadg_euler_update_3d(wadg_ctx *c, int K, const double *Jq, const double *VqPq,
+                         const double *VfPq, double fa, double fb, double fdt, double *rhsQ,
+                         double *resQ, double *Q, double *Qf) {
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({Jq, VqPq, VfPq, rhsQ, resQ, Q, Qf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_update<D_, N_, false>(c, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ,
+                                                         resQ, Q, Qf)));
+}
+
+int wadg_euler_update_3d_curved(wadg_ctx *c, int K, const double *Jq, const double *VqPq,
+                                const double *VfPq, double fa, double fb, double fdt,
+                                double *rhsQ, double *resQ, double *Q, double *Qf) {
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({Jq, VqPq, VfPq, rhsQ, resQ, Q, Qf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_update<D_, N_, true>(c, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ,
+                                                        resQ, Q, Qf)));
+}
+
+// ------------------------------------------------------------------ 2D
+int wadg_euler_vol_2d(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                      const double *nrJ, const double *nsJ, const double *Drq, const double *Dsq,
+                      const double *VqLq, const double *VfPq, const double *Q, const double *Qf,
+                      double *rhsQ, double *rhsQf) {
+  (void)Q; (void)vfgeo;
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_vol<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
+                                                      Dsq, nullptr, VqLq, VfPq, Qf, rhsQ,
+                                                      rhsQf)));
+}
+
+int wadg_euler_vol_2d_curved(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                             const double *nrJ, const double *nsJ, const double *Drq,
+                             const double *Dsq, const double *VqLq, const double *VfPq,
+                             const double *Q, const double *Qf, double *rhsQ, double *rhsQf) {
+  (void)Q;
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, vfgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_vol<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
+                                                     Dsq, nullptr, VqLq, VfPq, Qf, rhsQ,
+                                                     rhsQf)));
+}
+
+int wadg_euler_surf_2d(wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
+                       const double *VqLq, const double *Qf, const double *rhsQf, double *rhsQ) {
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_surf<D_, N_>(c, K, fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ)));
+}
+
+int wadg_euler_update_2d(wadg_ctx *c, int K, const double *Jq, const double *VqPq,
+                         const double *VfPq, double fa, double fb, double fdt, double *rhsQ,
+                         double *resQ, double *Q, double *Qf) {
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({Jq, VqPq, VfPq, rhsQ, resQ, Q, Qf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_update<D_, N_, false>(c, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ,
+                                                         resQ, Q, Qf)));
+}
+
+int wadg_euler_update_2d_curved(wadg_ctx *c, int K, const double *Jq, const double *VqPq,
+                                const double *VfPq, double fa, double fb, double fdt,
+                                double *rhsQ, double *resQ, double *Q, double *Qf) {
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({Jq, VqPq, VfPq, rhsQ, resQ, Q, Qf}))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_update<D_, N_, true>(c, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ,
+                                                        resQ, Q, Qf)));
+}
+
+}  // extern "C"

@@ -1,0 +1,205 @@
+// Device building blocks of the entropy-stable flux-differencing RHS:
+// compile-time element sizes, FP64 reciprocal, log-mean, two-point EC flux,
+// conservative <-> entropy variables.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wadg {
+
+// Element sizes of the reference's operator builder for cubature degree 2N
+// (tri_cubature / tet_cubature tables of node_data.h as used by
+// build_ref_ops_2D/3D, operators.cpp:104-341).
+template <int DIM, int N> struct Sizes;
+template <> struct Sizes<2, 1> { static constexpr int Np = 3,  Nq = 3,  Nfq = 2;  };
+template <> struct Sizes<2, 2> { static constexpr int Np = 6,  Nq = 6,  Nfq = 3;  };
+template <> struct Sizes<2, 3> { static constexpr int Np = 10, Nq = 12, Nfq = 4;  };
+template <> struct Sizes<2, 4> { static constexpr int Np = 15, Nq = 16, Nfq = 5;  };
+template <> struct Sizes<3, 1> { static constexpr int Np = 4,  Nq = 4,  Nfq = 3;  };
+template <> struct Sizes<3, 2> { static constexpr int Np = 10, Nq = 11, Nfq = 6;  };
+template <> struct Sizes<3, 3> { static constexpr int Np = 20, Nq = 23, Nfq = 12; };
+template <> struct Sizes<3, 4> { static constexpr int Np = 35, Nq = 44, Nfq = 16; };
+
+template <int DIM, int N> struct Elem {
+  static constexpr int Nfaces = DIM + 1;
+  static constexpr int Nq = Sizes<DIM, N>::Nq;
+  static constexpr int Nfq = Sizes<DIM, N>::Nfq;
+  static constexpr int NfqNf = Nfq * Nfaces;
+  static constexpr int Nfields = DIM + 2;
+  static constexpr int Nvgeo = DIM * DIM;
+  static constexpr int Nfgeo = DIM + 1;
+  static constexpr int NN = Nq + NfqNf;   // volume + face nodes
+  static constexpr int NS = DIM + 4;      // rho, velocity, beta, log rho, log beta
+};
+
+struct Phys {
+  double gamma;
+  double gm1;     // gamma - 1
+  double cbeta;   // 1 / (2 (gamma - 1))
+  double tau;     // LF penalty scale of the surface kernel
+};
+
+// 1/x: Newton-Raphson refinement (two steps, quadratic convergence) of the
+// hardware reciprocal estimate rcp.approx.ftz.f64.  Accurate to a few ulp for
+// the positive, normal-range arguments it is used on (sums of densities and
+// inverse temperatures, log differences).
+__device__ __forceinline__ double rcp(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  return y;
+}
+
+// Log-mean of a, b > 0: (a - b) / (log a - log b).
+//
+// The reference (Euler3Daffine.okl:43-71, Euler2D.okl:36-67) evaluates
+// (a + b) / (2F) with F = log(xi)/(2f), f = (xi-1)/(xi+1), xi = a/b, and
+// replaces F by its Taylor series F(u) = sum_k u^k/(2k+1), u = f^2, when u is
+// small.  Here log a and log b are computed once per node, so
+//   * for u < 1e-2 the series is used (degree 8 in u: truncation below 1e-18
+//     relative, so this branch is accurate to rounding over a wider range than
+//     the reference's 1e-4 / 1e-3 switch, where the log-difference would lose
+//     digits to cancellation);
+//   * otherwise (a+b)/(2F) = (a-b)/(log a - log b), where |log a - log b| >=
+//     0.2 keeps the cancellation error of the difference below ~1e-14.
+// Both branches agree with the reference's to rounding (parity tests hold
+// them to 1e-12 relative).
+__device__ __forceinline__ double polyF(double u) {  // sum_{k<=8} u^k/(2k+1)
+  double p = 1.0 / 17.0;
+  p = fma(p, u, 1.0 / 15.0);
+  p = fma(p, u, 1.0 / 13.0);
+  p = fma(p, u, 1.0 / 11.0);
+  p = fma(p, u, 1.0 / 9.0);
+  p = fma(p, u, 1.0 / 7.0);
+  p = fma(p, u, 1.0 / 5.0);
+  p = fma(p, u, 1.0 / 3.0);
+  return fma(p, u, 1.0);
+}
+// 1/F(u) to degree 8 (coefficients of the series reciprocal, exact rationals)
+__device__ __forceinline__ double polyG(double u) {
+  double p = -5472607916.0 / 488462349375.0;
+  p = fma(p, u, -25865068.0 / 1915538625.0);
+  p = fma(p, u, -10719068.0 / 638512875.0);
+  p = fma(p, u, -10196.0 / 467775.0);
+  p = fma(p, u, -428.0 / 14175.0);
+  p = fma(p, u, -44.0 / 945.0);
+  p = fma(p, u, -4.0 / 45.0);
+  p = fma(p, u, -1.0 / 3.0);
+  return fma(p, u, 1.0);
+}
+
+__device__ __forceinline__ double logmean(double a, double b, double la, double lb) {
+  const double d = a - b, s = a + b;
+  if (d * d < 1e-2 * (s * s)) {
+    const double f = d * rcp(s);
+    return 0.5 * s * polyG(f * f);
+  }
+  return d * rcp(la - lb);
+}
+
+// 1 / logmean(a, b), and 1/(a+b) through `isum`
+__device__ __forceinline__ double inv_logmean(double a, double b, double la, double lb,
+                                              double &isum) {
+  const double d = a - b, s = a + b;
+  isum = rcp(s);
+  if (d * d < 1e-2 * (s * s)) {
+    const double f = d * isum;
+    return 2.0 * isum * polyF(f * f);
+  }
+  return (la - lb) * rcp(d);
+}
+
+// Per-node state of the two-point flux: everything of euler3d_flux /
+// euler2d_flux (Euler3Daffine.okl:107-148, Euler2D.okl:139-161) that depends
+// on one node only.
+template <int DIM> struct NodeState {
+  double rho, vel[DIM], beta, lrho, lbeta;
+};
+
+// from conservative variables q[f*stride]; beta = rho / (2p)
+// (Euler3Daffine.okl:22-26 pfun/beta, Euler2D.okl:19-21)
+template <int DIM>
+__device__ __forceinline__ NodeState<DIM> node_state(const double *q, int stride, const Phys &P) {
+  NodeState<DIM> s;
+  s.rho = q[0];
+  const double ir = 1.0 / s.rho;
+  double kin = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.vel[d] = q[(1 + d) * stride] * ir;
+    kin = fma(s.vel[d], s.vel[d], kin);
+  }
+  const double E = q[(DIM + 1) * stride];
+  const double p = P.gm1 * (E - 0.5 * s.rho * kin);
+  s.beta = s.rho / (2.0 * p);
+  s.lrho = log(s.rho);
+  s.lbeta = log(s.beta);
+  return s;
+}
+
+// Chandrashekar's entropy-conservative flux F_S(a, b) contracted with the
+// direction n:  F.n  (the reference forms FxS, FyS, FzS and then
+// FxS*nx + FyS*ny + FzS*nz; this is the same sum regrouped):
+//   rholog = L(rho), betalog = L(beta), ubar = (ua+ub)/2,
+//   pa = rhoavg / (2 betaavg),  un = ubar.n,
+//   F0 = rholog un, Fm = F0 ubar + pa n,
+//   FE = (rholog/(2(gamma-1) betalog) + pa + rholog (ua.ub)/2) un
+// where ua.ub equals the reference's 2|ubar|^2 - avg(|u|^2).
+template <int DIM>
+__device__ __forceinline__ void ecflux_n(const NodeState<DIM> &a, const NodeState<DIM> &b,
+                                         const double *n, const Phys &P, double *F) {
+  double isb;
+  const double ibl = inv_logmean(a.beta, b.beta, a.lbeta, b.lbeta, isb);
+  const double rl = logmean(a.rho, b.rho, a.lrho, b.lrho);
+  const double pa = 0.5 * (a.rho + b.rho) * isb;
+  double ub[DIM], un = 0.0, vv = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    ub[d] = 0.5 * (a.vel[d] + b.vel[d]);
+    un = fma(ub[d], n[d], un);
+    vv = fma(a.vel[d], b.vel[d], vv);
+  }
+  const double f4 = fma(rl, fma(ibl, P.cbeta, 0.5 * vv), pa);
+  const double F0 = rl * un;
+  F[0] = F0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = fma(F0, ub[d], pa * n[d]);
+  F[DIM + 1] = f4 * un;
+}
+
+// conservative -> entropy variables (Euler3Daffine.okl:73-93 / Euler2D.okl:69-87)
+template <int DIM>
+__device__ __forceinline__ void VU(const double *U, double *V, const Phys &P) {
+  const double rho = U[0], E = U[DIM + 1];
+  double m2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) m2 = fma(U[1 + d], U[1 + d], m2);
+  const double rhoe = E - 0.5 * m2 / rho;
+  const double s = log(P.gm1 * rhoe / pow(rho, P.gamma));
+  const double irhoe = 1.0 / rhoe;
+  V[0] = (-E + rhoe * (P.gamma + 1.0 - s)) * irhoe;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) V[1 + d] = U[1 + d] * irhoe;
+  V[DIM + 1] = -rho * irhoe;
+}
+
+// entropy -> conservative variables (Euler3Daffine.okl:95-105 / Euler2D.okl:89-98)
+template <int DIM>
+__device__ __forceinline__ void UV(const double *V, double *U, const Phys &P) {
+  const double Vl = V[DIM + 1];
+  double vv = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) vv = fma(V[1 + d], V[1 + d], vv);
+  const double sV = P.gamma - V[0] + vv / (2.0 * Vl);
+  const double rhoe = pow(P.gm1 / pow(-Vl, P.gamma), 1.0 / P.gm1) * exp(-sV / P.gm1);
+  U[0] = -rhoe * Vl;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) U[1 + d] = rhoe * V[1 + d];
+  U[DIM + 1] = rhoe * (1.0 - vv / (2.0 * Vl));
+}
+
+}  // namespace wadg

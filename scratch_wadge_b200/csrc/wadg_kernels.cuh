@@ -1,0 +1,365 @@
+// The three kernels of one LSRK stage (volume, surface, update), templated on
+// dimension and degree.  One CTA handles E consecutive elements; everything an
+// element reads more than once is staged in shared memory.
+#pragma once
+
+#include "wadg_device.cuh"
+
+namespace wadg {
+
+// ---------------------------------------------------------------- volume
+// rhsQ_i = sum_j (Q_x F_S(u_i,u_j))_ij + 1/2 sum_f VqLq_if F_S(u_i,uf_f).nJ_f
+// rhsQf_f = -1/2 sum_j VfPq_fj F_S(uf_f,u_j).nJ_f
+// (Euler3Daffine.okl:152-417, Euler3D.okl:2123-2523, Euler2D.okl:235-1353)
+//
+// Prologue: one thread per node converts the staged conservative state into
+// the per-node flux state (rho, velocity, beta, log rho, log beta) once, so the
+// pair loops do no divisions by rho, no pressure recovery and no logarithms.
+// Rows: threads [0, E*Nq) own volume rows, threads [E*Nq, E*NN) own face rows;
+// each accumulates its row in registers in the reference's j order.
+template <int DIM, int N, bool CURVED, int E>
+struct VolCfg {
+  using El = Elem<DIM, N>;
+  static constexpr int threads = E * El::NN;
+  static constexpr size_t smem_state = sizeof(double) * E * El::NS * El::NN;
+  static constexpr size_t smem_geo = sizeof(double) * E * El::Nvgeo * (CURVED ? El::NN : 1);
+  static constexpr size_t smem = smem_state + smem_geo;
+};
+
+template <int DIM, int N, bool CURVED, int E>
+__global__ void __launch_bounds__(VolCfg<DIM, N, CURVED, E>::threads)
+vol_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
+           const double *__restrict__ nrJ, const double *__restrict__ nsJ,
+           const double *__restrict__ ntJ, const double *__restrict__ Drq,
+           const double *__restrict__ Dsq, const double *__restrict__ Dtq,
+           const double *__restrict__ VqLq, const double *__restrict__ VfPq,
+           const double *__restrict__ Qf, double *__restrict__ rhsQ,
+           double *__restrict__ rhsQf, Phys P) {
+  using El = Elem<DIM, N>;
+  constexpr int Nq = El::Nq, NfqNf = El::NfqNf, Nfq = El::Nfq, NN = El::NN, NS = El::NS;
+  constexpr int Nf = El::Nfields, NG = El::Nvgeo, NGN = CURVED ? NN : 1;
+  extern __shared__ double smem[];
+  double (*st)[NS][NN] = reinterpret_cast<double (*)[NS][NN]>(smem);
+  double (*sg)[NG][NGN] = reinterpret_cast<double (*)[NG][NGN]>(smem + E * NS * NN);
+
+  const int k0 = blockIdx.x * E;
+
+  for (int t = threadIdx.x; t < E * NN; t += blockDim.x) {
+    const int e = t / NN, n = t % NN, k = k0 + e;
+    if (k >= K) continue;
+    NodeState<DIM> s = (n < Nq) ? node_state<DIM>(rhsQ + (size_t)k * Nq * Nf + n, Nq, P)
+                                : node_state<DIM>(Qf + (size_t)k * NfqNf * Nf + (n - Nq), NfqNf, P);
+    st[e][0][n] = s.rho;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) st[e][1 + d][n] = s.vel[d];
+    st[e][DIM + 1][n] = s.beta;
+    st[e][DIM + 2][n] = s.lrho;
+    st[e][DIM + 3][n] = s.lbeta;
+    if (CURVED) {
+#pragma unroll
+      for (int c = 0; c < NG; ++c)
+        sg[e][c][n] = (n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
+                               : vfgeo[(size_t)k * NfqNf * NG + c * NfqNf + (n - Nq)];
+    } else if (n < NG) {
+      // affine: geometric factors of the first quadrature node (:205)
+      sg[e][n][0] = vgeo[(size_t)k * Nq * NG + n * Nq];
+    }
+  }
+  __syncthreads();
+
+  const int t = threadIdx.x;
+  const bool volrow = t < E * Nq;
+  const int e = volrow ? t / Nq : (t - E * Nq) / NfqNf;
+  const int row = volrow ? t % Nq : Nq + (t - E * Nq) % NfqNf;
+  const int k = k0 + e;
+  if (k >= K) return;
+
+  auto load = [&](int n) {
+    NodeState<DIM> s;
+    s.rho = st[e][0][n];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s.vel[d] = st[e][1 + d][n];
+    s.beta = st[e][DIM + 1][n];
+    s.lrho = st[e][DIM + 2][n];
+    s.lbeta = st[e][DIM + 3][n];
+    return s;
+  };
+  // direction G^T r for reference direction r (G rows: r-, s-, t-factors)
+  auto contract = [&](const double *G, const double *r, double *n) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      double v = 0.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) v = fma(G[a * DIM + d], r[a], v);
+      n[d] = v;
+    }
+  };
+
+  const NodeState<DIM> A = load(row);
+  double Gi[NG];
+#pragma unroll
+  for (int c = 0; c < NG; ++c) Gi[c] = CURVED ? sg[e][c][row] : sg[e][c][0];
+  double acc[Nf];
+#pragma unroll
+  for (int f = 0; f < Nf; ++f) acc[f] = 0.0;
+
+  if (volrow) {
+    const int i = row;
+    for (int j = 0; j < Nq; ++j) {
+      const NodeState<DIM> B = load(j);
+      double r[DIM], G[NG], nv[DIM], F[Nf];
+      r[0] = __ldg(Drq + i + j * Nq);
+      r[1] = __ldg(Dsq + i + j * Nq);
+      if (DIM == 3) r[DIM - 1] = __ldg(Dtq + i + j * Nq);
+#pragma unroll
+      for (int c = 0; c < NG; ++c) G[c] = CURVED ? 0.5 * (Gi[c] + sg[e][c][j]) : Gi[c];
+      contract(G, r, nv);
+      ecflux_n<DIM>(A, B, nv, P, F);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) acc[f] += F[f];
+    }
+    for (int j = 0; j < NfqNf; ++j) {
+      const NodeState<DIM> B = load(Nq + j);
+      const int fc = j / Nfq;
+      double r[DIM], G[NG], nv[DIM], F[Nf];
+      r[0] = __ldg(nrJ + fc * Nfq);
+      r[1] = __ldg(nsJ + fc * Nfq);
+      if (DIM == 3) r[DIM - 1] = __ldg(ntJ + fc * Nfq);
+#pragma unroll
+      for (int c = 0; c < NG; ++c) G[c] = CURVED ? 0.5 * (Gi[c] + sg[e][c][Nq + j]) : Gi[c];
+      contract(G, r, nv);
+      ecflux_n<DIM>(A, B, nv, P, F);
+      const double w = 0.5 * __ldg(VqLq + i + j * Nq);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) acc[f] = fma(w, F[f], acc[f]);
+    }
+    double *out = rhsQ + (size_t)k * Nq * Nf + i;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f * Nq] = acc[f];
+  } else {
+    const int i = row - Nq;
+    const int fc = i / Nfq;
+    double r[DIM];
+    r[0] = __ldg(nrJ + fc * Nfq);
+    r[1] = __ldg(nsJ + fc * Nfq);
+    if (DIM == 3) r[DIM - 1] = __ldg(ntJ + fc * Nfq);
+    double nv[DIM];
+    contract(Gi, r, nv);
+    for (int j = 0; j < Nq; ++j) {
+      const NodeState<DIM> B = load(j);
+      double F[Nf];
+      if (CURVED) {
+        double G[NG];
+#pragma unroll
+        for (int c = 0; c < NG; ++c) G[c] = 0.5 * (Gi[c] + sg[e][c][j]);
+        contract(G, r, nv);
+      }
+      ecflux_n<DIM>(A, B, nv, P, F);
+      const double w = -0.5 * __ldg(VfPq + i + j * NfqNf);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) acc[f] = fma(w, F[f], acc[f]);
+    }
+    double *out = rhsQf + (size_t)k * NfqNf * Nf + i;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f * NfqNf] = acc[f];
+  }
+}
+
+// ---------------------------------------------------------------- surface
+// sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam-,lam+) sJ (u+ - u-),
+// rhsQ += VqLq sfS   (Euler3D.okl:3242-3473, Euler2D.okl:1357-1495)
+template <int DIM, int N, int E>
+struct SurfCfg {
+  using El = Elem<DIM, N>;
+  static constexpr int threads = E * (El::NfqNf > El::Nq ? El::NfqNf : El::Nq);
+  static constexpr size_t smem = sizeof(double) * E * El::Nfields * El::NfqNf;
+};
+
+template <int DIM, int N, int E>
+__global__ void __launch_bounds__(SurfCfg<DIM, N, E>::threads)
+surf_kernel(int K, const double *__restrict__ fgeo, const uint32_t *__restrict__ mapPq,
+            const double *__restrict__ VqLq, const double *__restrict__ Qf,
+            const double *__restrict__ rhsQf, double *__restrict__ rhsQ, Phys P) {
+  using El = Elem<DIM, N>;
+  constexpr int Nq = El::Nq, NfqNf = El::NfqNf, Nf = El::Nfields, NFG = El::Nfgeo;
+  extern __shared__ double smem[];
+  double (*sf)[Nf][NfqNf] = reinterpret_cast<double (*)[Nf][NfqNf]>(smem);
+  const int k0 = blockIdx.x * E;
+
+  for (int t = threadIdx.x; t < E * NfqNf; t += blockDim.x) {
+    const int e = t / NfqNf, i = t % NfqNf, k = k0 + e;
+    if (k >= K) continue;
+    const size_t idM = i + (size_t)k * NfqNf * Nf;
+    const size_t idP = mapPq[i + (size_t)k * NfqNf];
+    const double *fg = fgeo + (size_t)k * NfqNf * NFG + i;
+    double nJ[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nJ[d] = fg[d * NfqNf];
+    const double sJ = fg[DIM * NfqNf];
+    double UM[Nf], UP[Nf];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) {
+      UM[f] = Qf[idM + f * NfqNf];
+      UP[f] = Qf[idP + f * NfqNf];
+    }
+    const NodeState<DIM> M = node_state<DIM>(UM, 1, P);
+    const NodeState<DIM> Pp = node_state<DIM>(UP, 1, P);
+    double F[Nf];
+    ecflux_n<DIM>(M, Pp, nJ, P, F);
+    // wave speeds |u| + sqrt(gamma p / rho), p = rho / (2 beta)
+    double kM = 0.0, kP = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      kM = fma(M.vel[d], M.vel[d], kM);
+      kP = fma(Pp.vel[d], Pp.vel[d], kP);
+    }
+    const double pM = P.gm1 * (UM[Nf - 1] - 0.5 * M.rho * kM);
+    const double pP = P.gm1 * (UP[Nf - 1] - 0.5 * Pp.rho * kP);
+    const double lamM = sqrt(kM) + sqrt(P.gamma * pM / M.rho);
+    const double lamP = sqrt(kP) + sqrt(P.gamma * pP / Pp.rho);
+    const double tau = (DIM == 3) ? P.tau : 1.0;
+    const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
+    const double *rf = rhsQf + idM;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) sf[e][f][i] = 0.5 * F[f] + rf[f * NfqNf] - Lfc * (UP[f] - UM[f]);
+  }
+  __syncthreads();
+
+  for (int t = threadIdx.x; t < E * Nq; t += blockDim.x) {
+    const int e = t / Nq, i = t % Nq, k = k0 + e;
+    if (k >= K) continue;
+    double val[Nf];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) val[f] = 0.0;
+    for (int j = 0; j < NfqNf; ++j) {
+      const double w = __ldg(VqLq + i + j * Nq);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) val[f] = fma(w, sf[e][f][j], val[f]);
+    }
+    double *out = rhsQ + (size_t)k * Nq * Nf + i;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f * Nq] += val[f];
+  }
+}
+
+// ---------------------------------------------------------------- update
+// affine (Euler3Daffine.okl:555-773, Euler2D.okl:1498-1725):
+//   r = -2 VqPq rhs / J; res = a res + dt r; Q += b res; v = V(Q);
+//   Qf = U(VfPq v); rhsQ = U(VqPq v)
+// WADG (Euler3D.okl:2527-2884, Euler2D.okl:1729-2282):
+//   r = VqPq((-2 VqPq rhs)/J); ...; v~ = VqPq((VqPq(v J))/J);
+//   Qf = U(VfPq v~); rhsQ = U(VqPq v~)
+template <int DIM, int N, bool CURVED, int E>
+struct UpdCfg {
+  using El = Elem<DIM, N>;
+  static constexpr int threads = E * El::Nq;
+  static constexpr size_t smem = sizeof(double) * 2 * E * El::Nfields * El::Nq;
+};
+
+template <int DIM, int N, bool CURVED, int E>
+__global__ void __launch_bounds__(UpdCfg<DIM, N, CURVED, E>::threads)
+update_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
+              const double *__restrict__ VfPq, double fa, double fb, double fdt,
+              double *__restrict__ rhsQ, double *__restrict__ resQ, double *__restrict__ Q,
+              double *__restrict__ Qf, Phys P) {
+  using El = Elem<DIM, N>;
+  constexpr int Nq = El::Nq, NfqNf = El::NfqNf, Nf = El::Nfields;
+  extern __shared__ double smem[];
+  double (*s)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
+  double (*sV)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
+  const int k0 = blockIdx.x * E;
+  const int kend = min(K - k0, E);
+
+  // the E elements' rhsQ blocks are one contiguous range: copy it flat
+  const double *src = rhsQ + (size_t)k0 * Nf * Nq;
+  for (int t = threadIdx.x; t < kend * Nf * Nq; t += blockDim.x) (&s[0][0][0])[t] = src[t];
+  __syncthreads();
+
+  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
+  const bool valid = e < kend;
+  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
+
+  auto matvec = [&](const double *Op, int ld, int row, double (*X)[Nq], double *out) {
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f] = 0.0;
+    for (int j = 0; j < Nq; ++j) {
+      const double w = __ldg(Op + row + j * ld);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) out[f] = fma(w, X[f][j], out[f]);
+    }
+  };
+
+  double r[Nf];
+  if (CURVED) {
+    if (valid) {
+      matvec(VqPq, Nq, i, s[e], r);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) sV[e][f][i] = -2.0 * r[f] / Jqi;
+    }
+    __syncthreads();
+    if (valid) matvec(VqPq, Nq, i, sV[e], r);
+  } else if (valid) {
+    matvec(VqPq, Nq, i, s[e], r);
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) r[f] = -2.0 * r[f] / Jqi;
+  }
+
+  double V[Nf];
+  if (valid) {
+    const size_t id = (size_t)k * Nq * Nf + i;
+    double U[Nf];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) {
+      double res = resQ[id + f * Nq];
+      res = fa * res + fdt * r[f];
+      resQ[id + f * Nq] = res;
+      U[f] = Q[id + f * Nq] + fb * res;
+      Q[id + f * Nq] = U[f];
+    }
+    VU<DIM>(U, V, P);
+  }
+
+  double (*X)[Nf][Nq] = sV;  // what the final projection reads
+  if (CURVED) {
+    __syncthreads();  // everyone is done reading s (first matvec)
+    if (valid)
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) s[e][f][i] = V[f] * Jqi;
+    __syncthreads();
+    if (valid) {
+      matvec(VqPq, Nq, i, s[e], r);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) sV[e][f][i] = r[f] / Jqi;
+    }
+    __syncthreads();
+    if (valid) matvec(VqPq, Nq, i, sV[e], r);
+    __syncthreads();
+    if (valid)
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) s[e][f][i] = r[f];
+    X = s;
+  } else {
+    if (valid)
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) sV[e][f][i] = V[f];
+  }
+  __syncthreads();
+  if (!valid) return;
+
+  for (int ii = i; ii < NfqNf; ii += Nq) {
+    double Vf[Nf], Uf[Nf];
+    matvec(VfPq, NfqNf, ii, X[e], Vf);
+    UV<DIM>(Vf, Uf, P);
+    double *out = Qf + (size_t)k * NfqNf * Nf + ii;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f * NfqNf] = Uf[f];
+  }
+  double Vq[Nf], Uq[Nf];
+  matvec(VqPq, Nq, i, X[e], Vq);
+  UV<DIM>(Vq, Uq, P);
+  double *out = rhsQ + (size_t)k * Nq * Nf + i;
+#pragma unroll
+  for (int f = 0; f < Nf; ++f) out[f * Nq] = Uq[f];
+}
+
+}  // namespace wadg
