@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -68,6 +69,50 @@ int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo
   return after_launch("vol kernel");
 }
 
+// warps per CTA of vol2: as many as fit in 227 KB of shared memory (<= 8)
+template <int DIM, int N, bool CURVED>
+constexpr int vol2W() {
+  using C1 = Vol2Cfg<DIM, N, CURVED, 1>;
+  constexpr size_t fixed = sizeof(double) * (C1::nD + 2 * C1::nW + Elem<DIM, N>::Nfaces * DIM);
+  constexpr size_t per_warp = C1::smem - fixed;
+  constexpr size_t w = (227 * 1024 - fixed) / per_warp;
+  return w >= 8 ? 8 : (w < 1 ? 1 : (int)w);
+}
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int DIM, int N, bool CURVED>
+int launch_vol2(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+                const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
+                const double *Qf, double *rhsQ, double *rhsQf) {
+  constexpr int W = vol2W<DIM, N, CURVED>();
+  using C = Vol2Cfg<DIM, N, CURVED, W>;
+  static_assert(C::smem <= 227 * 1024, "vol2 does not fit in shared memory");
+  auto kern = vol2_kernel<DIM, N, CURVED, W>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    if (e != cudaSuccess) return cuda_check(e, "vol2 smem attribute");
+    attr = true;
+  }
+  const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
+  const int batches = (K + C::E - 1) / C::E;
+  const int grid = batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
+  kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
+                                                  VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
+  return after_launch("vol2 kernel");
+}
+
 template <int DIM, int N>
 int launch_surf(const wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
                 const double *VqLq, const double *Qf, const double *rhsQf, double *rhsQ) {
@@ -89,6 +134,29 @@ int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq
   update_kernel<DIM, N, CURVED, E><<<grid, C::threads, C::smem, c->stream>>>(
       K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf, c->phys);
   return after_launch("update kernel");
+}
+
+// The volume kernel used by the entry points: vol2 (each volume-face pair
+// once) by default; WADG_VOL_KERNEL=rows selects the row-per-thread kernel.
+int vol_variant() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("WADG_VOL_KERNEL");
+    v = (e && strcmp(e, "rows") == 0) ? 1 : 2;
+  }
+  return v;
+}
+
+template <int DIM, int N, bool CURVED>
+int vol_impl(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+             const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+             const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
+             const double *Qf, double *rhsQ, double *rhsQf) {
+  if (vol_variant() == 1)
+    return launch_vol<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
+                                      Qf, rhsQ, rhsQf);
+  return launch_vol2<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
+                                     Qf, rhsQ, rhsQf);
 }
 
 // (dim, N) -> template instantiation
@@ -205,8 +273,8 @@ int wadg_euler_vol_3d(wadg_ctx *c, int K, const double *vgeo, const double *vfge
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (launch_vol<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
-                                                      Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
+  WADG_DISPATCH(c, return (vol_impl<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
+                                                    Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
 int wadg_euler_vol_3d_curved(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
@@ -219,8 +287,8 @@ int wadg_euler_vol_3d_curved(wadg_ctx *c, int K, const double *vgeo, const doubl
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (launch_vol<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
-                                                     Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
+  WADG_DISPATCH(c, return (vol_impl<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
+                                                   Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
 int wadg_euler_surf_3d(wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
@@ -264,9 +332,8 @@ int wadg_euler_vol_2d(wadg_ctx *c, int K, const double *vgeo, const double *vfge
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (launch_vol<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
-                                                      Dsq, nullptr, VqLq, VfPq, Qf, rhsQ,
-                                                      rhsQf)));
+  WADG_DISPATCH(c, return (vol_impl<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
+                                                    Dsq, nullptr, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
 int wadg_euler_vol_2d_curved(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
@@ -278,9 +345,8 @@ int wadg_euler_vol_2d_curved(wadg_ctx *c, int K, const double *vgeo, const doubl
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, vfgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (launch_vol<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
-                                                     Dsq, nullptr, VqLq, VfPq, Qf, rhsQ,
-                                                     rhsQf)));
+  WADG_DISPATCH(c, return (vol_impl<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
+                                                   Dsq, nullptr, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
 int wadg_euler_surf_2d(wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,

@@ -155,12 +155,28 @@ def hmin(geo):
     return float(np.min(geo.Jq.min(axis=1) / sJ.max(axis=1)))
 
 
-def time_step(geo, CFL, N, FinalTime=None, nsteps=None):
+def max_wave_speed(Q, gamma=1.4):
+    """max over nodes of |u| + sqrt(gamma p / rho); Q in kernel layout."""
+    dim = Q.shape[1] - 2
+    rho, E = Q[:, 0], Q[:, -1]
+    u2 = sum((Q[:, 1 + d] / rho) ** 2 for d in range(dim))
+    p = (gamma - 1.0) * (E - 0.5 * rho * u2)
+    return float(np.max(np.sqrt(u2) + np.sqrt(gamma * p / rho)))
+
+
+def time_step(geo, CFL, N, FinalTime=None, nsteps=None, wave_speed=None):
     """dt = CFL*hmin/C_N (euler.c:4180-4193); with FinalTime, Nsteps =
-    ceil(T/dt) and dt = T/Nsteps (euler.c:3680-3688)."""
+    ceil(T/dt) and dt = T/Nsteps (euler.c:3680-3688).
+
+    The reference's formula carries no wave speed (it assumes one of order 1).
+    With ``wave_speed`` the step is divided by it: the Taylor-Green state
+    (p0 = 100/gamma, sound speed ~10) runs the reference's own kernels into
+    NaN within two steps at CFL 0.5 otherwise."""
     dim = geo.ops.dim
     CN = (N + 1) * (N + 2) / 2 if dim == 2 else (N + 1) * (N + 3) / 3
     dt = CFL * hmin(geo) / CN
+    if wave_speed is not None:
+        dt /= wave_speed
     if FinalTime is not None:
         n = int(math.ceil(FinalTime / dt))
         return FinalTime / n, n
