@@ -12,6 +12,7 @@
 
 #include "../../include/wadg.h"
 #include "wadg_kernels.cuh"
+#include "wadg_vol.cuh"
 
 using namespace wadg;
 
@@ -69,14 +70,14 @@ int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo
   return after_launch("vol kernel");
 }
 
-// warps per CTA of vol2: as many as fit in 227 KB of shared memory (<= 8)
+// warps per CTA of the pair-scheduled volume kernel: an even count, as many
+// as fit in 227 KB of shared memory, at most 12 (register budget ~170/thread)
 template <int DIM, int N, bool CURVED>
-constexpr int vol2W() {
-  using C1 = Vol2Cfg<DIM, N, CURVED, 1>;
-  constexpr size_t fixed = sizeof(double) * (C1::nD + 2 * C1::nW + Elem<DIM, N>::Nfaces * DIM);
-  constexpr size_t per_warp = C1::smem - fixed;
-  constexpr size_t w = (227 * 1024 - fixed) / per_warp;
-  return w >= 8 ? 8 : (w < 1 ? 1 : (int)w);
+constexpr int volpairsW() {
+  using C = VolPairsCfg<DIM, N, CURVED, 2>;
+  constexpr size_t per_warp = C::per_elem * VolTile<DIM, N>::G / C::H;
+  constexpr size_t w = (227 * 1024 - C::fixed) / per_warp;
+  return w >= 12 ? 12 : (w < 2 ? 2 : (int)(w & ~size_t(1)));
 }
 
 int num_sms() {
@@ -91,18 +92,18 @@ int num_sms() {
 }
 
 template <int DIM, int N, bool CURVED>
-int launch_vol2(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
-                const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
-                const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
-                const double *Qf, double *rhsQ, double *rhsQf) {
-  constexpr int W = vol2W<DIM, N, CURVED>();
-  using C = Vol2Cfg<DIM, N, CURVED, W>;
-  static_assert(C::smem <= 227 * 1024, "vol2 does not fit in shared memory");
-  auto kern = vol2_kernel<DIM, N, CURVED, W>;
+int launch_vol_pairs(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                     const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+                     const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
+                     const double *Qf, double *rhsQ, double *rhsQf) {
+  constexpr int W = volpairsW<DIM, N, CURVED>();
+  using C = VolPairsCfg<DIM, N, CURVED, W>;
+  static_assert(C::smem <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
+  auto kern = vol_pairs_kernel<DIM, N, CURVED, W>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-    if (e != cudaSuccess) return cuda_check(e, "vol2 smem attribute");
+    if (e != cudaSuccess) return cuda_check(e, "volume kernel smem attribute");
     attr = true;
   }
   const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
@@ -110,7 +111,7 @@ int launch_vol2(const wadg_ctx *c, int K, const double *vgeo, const double *vfge
   const int grid = batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
   kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
                                                   VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
-  return after_launch("vol2 kernel");
+  return after_launch("volume kernel");
 }
 
 template <int DIM, int N>
@@ -136,8 +137,8 @@ int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq
   return after_launch("update kernel");
 }
 
-// The volume kernel used by the entry points: vol2 (each volume-face pair
-// once) by default; WADG_VOL_KERNEL=rows selects the row-per-thread kernel.
+// The volume kernel used by the entry points: vol_pairs (each volume-face
+// pair once) by default; WADG_VOL_KERNEL=rows selects the row-per-thread kernel.
 int vol_variant() {
   static int v = -1;
   if (v < 0) {
@@ -155,8 +156,8 @@ int vol_impl(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
   if (vol_variant() == 1)
     return launch_vol<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
                                       Qf, rhsQ, rhsQf);
-  return launch_vol2<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
-                                     Qf, rhsQ, rhsQf);
+  return launch_vol_pairs<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq,
+                                          VfPq, Qf, rhsQ, rhsQf);
 }
 
 // (dim, N) -> template instantiation

@@ -363,267 +363,3 @@ update_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ V
 }
 
 }  // namespace wadg
-
-namespace wadg {
-
-// ---------------------------------------------------------------- volume v2
-// Same mathematics as vol_kernel, organised so that every volume-face pair
-// (i, f) is evaluated once: F_S(u_i, uf_f).nJ_f feeds both the volume row i
-// (weight 1/2 VqLq_if) and the face row f (weight -1/2 VfPq_fi).  The
-// reference evaluates it twice, once per row (Euler3Daffine.okl:327-362 and
-// :387-406); the flux is symmetric, so the sums are the same.
-//
-// Work layout.  A group of L lanes owns one element; lane l owns the R volume
-// rows i = l + L*r (register accumulators).  Volume-volume pairs: every lane
-// walks j = 0..Nq-1 (the column state is a broadcast within the group).
-// Volume-face pairs: at step s lane l takes face node f = (l + s) mod NfqNf,
-// so the L lanes of a group always touch L distinct face rows; each lane adds
-// its R contributions to the face row's shared-memory accumulator, and a
-// __syncwarp between steps orders the read-modify-writes.  The schedule is
-// fixed, so the result is deterministic (no atomics).
-//
-// Persistent CTAs: the operator tables are staged in shared memory once per
-// CTA, the weights in a rotated layout [r][s][l] so that the lanes of a step
-// read consecutive words.
-template <int DIM, int N> struct VolTile {
-  using El = Elem<DIM, N>;
-  static constexpr int Lraw = (El::Nq + 2) / 3;
-  static constexpr int L = Lraw <= 1 ? 1 : Lraw <= 2 ? 2 : Lraw <= 4 ? 4 : Lraw <= 8 ? 8 : Lraw <= 16 ? 16 : 32;
-  static constexpr int R = (El::Nq + L - 1) / L;
-  static constexpr int G = 32 / L;  // elements per warp
-  static_assert(El::NfqNf >= L, "face schedule needs NfqNf >= L");
-};
-
-template <int DIM, int N, bool CURVED, int W>
-struct Vol2Cfg {
-  using El = Elem<DIM, N>;
-  using T = VolTile<DIM, N>;
-  static constexpr int threads = 32 * W;
-  static constexpr int E = W * T::G;  // elements per CTA batch
-  static constexpr int pad8(int x) { return ((x + 7) / 16) * 16 + 8; }  // == 8 mod 16
-  static constexpr int NGS = CURVED ? El::Nvgeo : 0;               // geofacs per node
-  static constexpr int SE = pad8((El::NS + NGS) * El::NN);          // state stride / element
-  static constexpr int SA = pad8(El::Nfields * El::NfqNf);          // face acc stride
-  static constexpr int SN = El::Nfaces * DIM + El::Nvgeo;           // face normals + G (affine)
-  static constexpr int nD = DIM * El::Nq * El::Nq;
-  static constexpr int nW = T::R * El::NfqNf * T::L;
-  static constexpr size_t smem =
-      sizeof(double) * (size_t)(nD + 2 * nW + El::Nfaces * DIM + E * (SE + SA + SN));
-};
-
-template <int DIM, int N, bool CURVED, int W>
-__global__ void __launch_bounds__(32 * W)
-vol2_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
-            const double *__restrict__ nrJ, const double *__restrict__ nsJ,
-            const double *__restrict__ ntJ, const double *__restrict__ Drq,
-            const double *__restrict__ Dsq, const double *__restrict__ Dtq,
-            const double *__restrict__ VqLq, const double *__restrict__ VfPq,
-            const double *__restrict__ Qf, double *__restrict__ rhsQ,
-            double *__restrict__ rhsQf, Phys P) {
-  using El = Elem<DIM, N>;
-  using T = VolTile<DIM, N>;
-  using C = Vol2Cfg<DIM, N, CURVED, W>;
-  constexpr int Nq = El::Nq, NF = El::NfqNf, Nfq = El::Nfq, NN = El::NN, NS = El::NS;
-  constexpr int Nf = El::Nfields, NG = El::Nvgeo, L = T::L, R = T::R, G = T::G, E = C::E;
-  constexpr int SE = C::SE, SA = C::SA, SN = C::SN;
-
-  extern __shared__ double smem[];
-  double *sD = smem;                       // Drq | Dsq | Dtq, column-major
-  double *sW1 = sD + C::nD;                // [R][NF][L]  1/2 VqLq(i, f)
-  double *sW2 = sW1 + C::nW;               // [R][NF][L] -1/2 VfPq(f, i)
-  double *sNr = sW2 + C::nW;               // reference normals [Nfaces][DIM]
-  double *sSt = sNr + El::Nfaces * DIM;    // [E][SE]   node states (+ geofacs)
-  double *sAcc = sSt + E * SE;             // [E][SA]   face-row accumulators
-  double *sNrm = sAcc + E * SA;            // [E][SN]   per-face nJ (affine) + G
-
-  const int tid = threadIdx.x;
-  for (int t = tid; t < Nq * Nq; t += blockDim.x) {
-    sD[t] = Drq[t];
-    sD[Nq * Nq + t] = Dsq[t];
-    if (DIM == 3) sD[2 * Nq * Nq + t] = Dtq[t];
-  }
-  for (int t = tid; t < C::nW; t += blockDim.x) {
-    const int l = t % L, s = (t / L) % NF, r = t / (L * NF);
-    const int i = l + L * r;
-    int f = l + s;
-    if (f >= NF) f -= NF;
-    sW1[t] = i < Nq ? 0.5 * VqLq[i + f * Nq] : 0.0;
-    sW2[t] = i < Nq ? -0.5 * VfPq[f + i * NF] : 0.0;
-  }
-  for (int t = tid; t < El::Nfaces; t += blockDim.x) {
-    sNr[t * DIM + 0] = nrJ[t * Nfq];
-    sNr[t * DIM + 1] = nsJ[t * Nfq];
-    if (DIM == 3) sNr[t * DIM + 2] = ntJ[t * Nfq];
-  }
-
-  const int warp = tid >> 5, lane = tid & 31;
-  const int g = lane / L, l = lane % L;
-  const int e = warp * G + g;
-
-  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
-    __syncthreads();  // tables ready / previous batch done with shared memory
-    // ---- node states of the batch (one thread per node)
-    for (int t = tid; t < E * NN; t += blockDim.x) {
-      const int ee = t / NN, n = t % NN, k = k0 + ee;
-      if (k >= K) continue;
-      const NodeState<DIM> s = (n < Nq) ? node_state<DIM>(rhsQ + (size_t)k * Nq * Nf + n, Nq, P)
-                                        : node_state<DIM>(Qf + (size_t)k * NF * Nf + (n - Nq), NF, P);
-      double *st = sSt + ee * SE;
-      st[0 * NN + n] = s.rho;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = s.vel[d];
-      st[(DIM + 1) * NN + n] = s.beta;
-      st[(DIM + 2) * NN + n] = s.lrho;
-      st[(DIM + 3) * NN + n] = s.lbeta;
-      if (CURVED) {
-#pragma unroll
-        for (int c = 0; c < NG; ++c)
-          st[(NS + c) * NN + n] = (n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
-                                           : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
-      }
-    }
-    for (int t = tid; t < E * SA; t += blockDim.x) sAcc[t] = 0.0;
-    if (!CURVED) {
-      for (int t = tid; t < E; t += blockDim.x) {
-        const int k = k0 + t;
-        if (k >= K) continue;
-        double Gk[NG];
-#pragma unroll
-        for (int c = 0; c < NG; ++c) Gk[c] = vgeo[(size_t)k * Nq * NG + c * Nq];  // node 0 (:205)
-        double *nm = sNrm + t * SN;
-#pragma unroll
-        for (int c = 0; c < NG; ++c) nm[El::Nfaces * DIM + c] = Gk[c];
-        for (int fc = 0; fc < El::Nfaces; ++fc)
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            double v = 0.0;
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) v = fma(Gk[a * DIM + d], sNr[fc * DIM + a], v);
-            nm[fc * DIM + d] = v;
-          }
-      }
-    }
-    __syncthreads();
-
-    const int k = k0 + e;
-    const bool kval = k < K;
-    const double *st = sSt + e * SE;
-    double *acc_f = sAcc + e * SA;
-    auto load = [&](int n) {
-      NodeState<DIM> s;
-      s.rho = st[n];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) s.vel[d] = st[(1 + d) * NN + n];
-      s.beta = st[(DIM + 1) * NN + n];
-      s.lrho = st[(DIM + 2) * NN + n];
-      s.lbeta = st[(DIM + 3) * NN + n];
-      return s;
-    };
-
-    NodeState<DIM> A[R];
-    bool rv[R];
-    double acc[R][Nf];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = l + L * r;
-      rv[r] = kval && i < Nq;
-      A[r] = load(rv[r] ? i : 0);
-#pragma unroll
-      for (int q = 0; q < Nf; ++q) acc[r][q] = 0.0;
-    }
-    double Ge[NG];
-    if (!CURVED) {
-#pragma unroll
-      for (int c = 0; c < NG; ++c) Ge[c] = sNrm[e * SN + El::Nfaces * DIM + c];
-    }
-
-    // ---- volume-volume pairs (reference j order)
-    if (kval) {
-      for (int j = 0; j < Nq; ++j) {
-        const NodeState<DIM> B = load(j);
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          if (!rv[r]) continue;
-          const int i = l + L * r;
-          double rr[DIM], nv[DIM], F[Nf];
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) rr[a] = sD[a * Nq * Nq + i + j * Nq];
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            double v = 0.0;
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) {
-              const double gad = CURVED ? 0.5 * (st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + j])
-                                        : Ge[a * DIM + d];
-              v = fma(gad, rr[a], v);
-            }
-            nv[d] = v;
-          }
-          ecflux_n<DIM>(A[r], B, nv, P, F);
-#pragma unroll
-          for (int q = 0; q < Nf; ++q) acc[r][q] += F[q];
-        }
-      }
-    }
-
-    // ---- volume-face pairs, each evaluated once (staggered face schedule)
-    for (int s = 0; s < NF; ++s) {
-      int f = l + s;
-      if (f >= NF) f -= NF;
-      if (kval) {
-        const NodeState<DIM> B = load(Nq + f);
-        const int fc = f / Nfq;
-        double nv[DIM];
-        if (!CURVED) {
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) nv[d] = sNrm[e * SN + fc * DIM + d];
-        }
-        double af[Nf];
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) af[q] = 0.0;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          if (!rv[r]) continue;
-          if (CURVED) {
-            const int i = l + L * r;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-              double v = 0.0;
-#pragma unroll
-              for (int a = 0; a < DIM; ++a)
-                v = fma(0.5 * (st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + Nq + f]),
-                        sNr[fc * DIM + a], v);
-              nv[d] = v;
-            }
-          }
-          double F[Nf];
-          ecflux_n<DIM>(A[r], B, nv, P, F);
-          const double w1 = sW1[(r * NF + s) * L + l];
-          const double w2 = sW2[(r * NF + s) * L + l];
-#pragma unroll
-          for (int q = 0; q < Nf; ++q) {
-            acc[r][q] = fma(w1, F[q], acc[r][q]);
-            af[q] = fma(w2, F[q], af[q]);
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) acc_f[q * NF + f] += af[q];
-      }
-      __syncwarp();
-    }
-
-    if (kval) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (!rv[r]) continue;
-        double *out = rhsQ + (size_t)k * Nq * Nf + l + L * r;
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) out[q * Nq] = acc[r][q];
-      }
-      double *outf = rhsQf + (size_t)k * NF * Nf;
-      for (int t = l; t < NF * Nf; t += L) outf[t] = acc_f[t];
-    }
-  }
-}
-
-}  // namespace wadg
