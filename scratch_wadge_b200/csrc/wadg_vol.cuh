@@ -43,10 +43,15 @@ struct VolPairsCfg {
   static constexpr int H = 2;                         // warps per element group
   static constexpr int threads = 32 * W;
   static constexpr int E = (W / H) * T::G;            // elements per batch
-  static constexpr int pad8(int x) { return ((x + 7) / 16) * 16 + 8; }  // == 8 mod 16
+  // element strides in doubles: the state stride is 4 mod 8 and the stride of
+  // an element's pair of face accumulators (H*SA) is 4 mod 8, so the G groups
+  // of a warp start 8 banks apart (conflict-free broadcasts, two wavefronts
+  // for a step's consecutive face rows)
+  static constexpr int pad4of8(int x) { return ((x + 3) / 8) * 8 + 4; }   // == 4 mod 8
+  static constexpr int pad2of4(int x) { return ((x + 1) / 4) * 4 + 2; }   // == 2 mod 4
   static constexpr int NGS = CURVED ? El::Nvgeo : 0;  // geometric factors per node
-  static constexpr int SE = pad8((El::NS + NGS) * El::NN);
-  static constexpr int SA = pad8(El::Nfields * El::NfqNf);
+  static constexpr int SE = pad4of8((El::NS + NGS) * El::NN);
+  static constexpr int SA = pad2of4(El::Nfields * El::NfqNf);
   static constexpr int SN = El::Nfaces * DIM + El::Nvgeo;
   static constexpr int nD = DIM * El::Nq * El::Nq;
   static constexpr int nW = T::R * El::NfqNf * T::L;
