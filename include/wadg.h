@@ -136,6 +136,35 @@ int wadg_euler_update_2d_curved(wadg_ctx *ctx, int K, const double *Jq,
                                 double fa, double fb, double fdt, double *rhsQ,
                                 double *resQ, double *Q, double *Qf);
 
+/* ------------------------------------------------------------ fused stage
+ * One LSRK stage -- vol, surf and update of the kernels above -- in a single
+ * launch (rk_step, euler.c:3610-3666, with rhsQf and the volume RHS kept on
+ * chip).  No single-kernel counterpart in the reference.  The entropy-
+ * projected state is read from (rhsQ_in, Qf_in) and written to (rhsQ_out,
+ * Qf_out), which must be distinct buffers (a neighbour's trace of the current
+ * stage is still being read while the next stage's is written); Q and resQ
+ * are updated in place.  curved = 0: Euler3Daffine / euler_vol_2d algebra;
+ * 1: Euler3D curved / WADG. */
+int wadg_euler_stage_3d(wadg_ctx *ctx, int K, int curved, const double *vgeo,
+                        const double *vfgeo, const double *fgeo,
+                        const uint32_t *mapPq, const double *nrJ,
+                        const double *nsJ, const double *ntJ, const double *Drq,
+                        const double *Dsq, const double *Dtq,
+                        const double *VqLq, const double *VfPq,
+                        const double *VqPq, const double *Jq, double fa,
+                        double fb, double fdt, const double *rhsQ_in,
+                        const double *Qf_in, double *Q, double *resQ,
+                        double *rhsQ_out, double *Qf_out);
+int wadg_euler_stage_2d(wadg_ctx *ctx, int K, int curved, const double *vgeo,
+                        const double *vfgeo, const double *fgeo,
+                        const uint32_t *mapPq, const double *nrJ,
+                        const double *nsJ, const double *Drq, const double *Dsq,
+                        const double *VqLq, const double *VfPq,
+                        const double *VqPq, const double *Jq, double fa,
+                        double fb, double fdt, const double *rhsQ_in,
+                        const double *Qf_in, double *Q, double *resQ,
+                        double *rhsQ_out, double *Qf_out);
+
 /* ------------------------------------------------------------ host driver
  * The reference's app_t / rk_step / rk_run (euler.c:2607-2796, 3610-3738)
  * over device buffers owned by the library.  Host arrays are copied once at
@@ -178,6 +207,10 @@ int wadg_app_solve_host(wadg_app *app, const double *Q0, const double *rhsQ0,
                         int nsteps, double *Q, double *rhsQ, double *Qf,
                         double *resQ);
 int wadg_app_sync(wadg_app *app);
+/* fused != 0 (the default): wadg_rk_step / wadg_rk_run launch the fused stage
+ * kernel (one launch per stage, ping-pong state buffers); 0: the three
+ * reference kernels per stage.  Results agree to rounding. */
+int wadg_app_set_fused(wadg_app *app, int fused);
 /* device pointers of the state arrays (for zero-copy use and testing) */
 int wadg_app_state_ptrs(wadg_app *app, double **Q, double **rhsQ, double **Qf,
                         double **resQ, double **rhsQf);
@@ -188,6 +221,9 @@ int wadg_app_time_run(wadg_app *app, double dt, int nsteps, int use_graph,
 /* Time each of the three kernels over `nstages` stages with CUDA events
  * around every launch; ms[0..2] = total vol, surf, update time. */
 int wadg_app_time_kernels(wadg_app *app, double dt, int nstages, float *ms);
+/* Time `nstages` fused stage launches (CUDA events around the sequence);
+ * ms receives the total. */
+int wadg_app_time_stage(wadg_app *app, double dt, int nstages, float *ms);
 
 /* ------------------------------------------------------------ measurement
  * FP64 FMA throughput of the current GPU (the denominator of the volume

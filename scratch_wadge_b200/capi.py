@@ -73,6 +73,12 @@ def lib():
         L.wadg_app_set_state.argtypes = [v, v, v, v, v]
         L.wadg_app_get_state.argtypes = [v, v, v, v, v]
         L.wadg_app_state_ptrs.argtypes = [v] + [ctypes.POINTER(ctypes.c_void_p)] * 5
+        L.wadg_euler_stage_3d.argtypes = [v, i, i] + [v] * 14 + [d, d, d] + [v] * 6
+        L.wadg_euler_stage_2d.argtypes = [v, i, i] + [v] * 12 + [d, d, d] + [v] * 6
+        L.wadg_app_set_fused.argtypes = [v, i]
+        L.wadg_app_time_stage.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
+        L.wadg_probe_fp64_fma.argtypes = [v, i, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_float)]
         L.wadg_app_create.argtypes = [ctypes.POINTER(Params), i, i, ctypes.POINTER(HostData),
                                       ctypes.POINTER(ctypes.c_void_p)]
         L.wadg_ctx_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]
@@ -129,6 +135,19 @@ class Context:
         L = lib()
         fn = L.wadg_euler_surf_3d if self.ops.dim == 3 else L.wadg_euler_surf_2d
         check(fn(self.h, K, fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ), "surf")
+
+    def stage(self, curved, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
+              VqPq, Jq, fa, fb, fdt, rhsQ_in, Qf_in, Q, resQ, rhsQ_out, Qf_out):
+        """The fused stage (wadg_euler_stage_3d/_2d): vol + surf + update."""
+        L = lib()
+        if self.ops.dim == 3:
+            check(L.wadg_euler_stage_3d(self.h, K, int(curved), vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ,
+                                        Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, rhsQ_in,
+                                        Qf_in, Q, resQ, rhsQ_out, Qf_out), "stage")
+        else:
+            check(L.wadg_euler_stage_2d(self.h, K, int(curved), vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                        Drq, Dsq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, rhsQ_in, Qf_in,
+                                        Q, resQ, rhsQ_out, Qf_out), "stage")
 
     def update(self, curved, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf):
         L = lib()
@@ -211,6 +230,15 @@ class App:
     def time_run(self, dt, nsteps, graph=True):
         ms = ctypes.c_float()
         check(lib().wadg_app_time_run(self.h, dt, nsteps, int(graph), ctypes.byref(ms)), "time_run")
+        return ms.value
+
+    def set_fused(self, fused: bool):
+        """fused stage kernel (default) or the three reference kernels per stage"""
+        check(lib().wadg_app_set_fused(self.h, int(fused)), "set_fused")
+
+    def time_stage(self, dt, nstages):
+        ms = ctypes.c_float()
+        check(lib().wadg_app_time_stage(self.h, dt, nstages, ctypes.byref(ms)), "time_stage")
         return ms.value
 
     def time_kernels(self, dt, nstages):

@@ -46,11 +46,16 @@ struct wadg_app {
   uint32_t *mapPq = nullptr;
   double *nrJ = nullptr, *nsJ = nullptr, *ntJ = nullptr, *Drq = nullptr, *Dsq = nullptr,
          *Dtq = nullptr, *Drstq = nullptr, *VqLq = nullptr, *VqPq = nullptr, *VfPq = nullptr;
-  // solver state
-  double *Q = nullptr, *rhsQ = nullptr, *Qf = nullptr, *resQ = nullptr, *rhsQf = nullptr;
-  // graph of one time step
-  cudaGraphExec_t graph = nullptr;
-  double graph_dt = 0.0;
+  // solver state; the entropy-projected state (rhsQ, Qf) is double-buffered
+  // for the fused stage kernel: buffer `cur` holds the current stage's
+  double *Q = nullptr, *resQ = nullptr, *rhsQf = nullptr;
+  double *uq[2] = {nullptr, nullptr}, *uf[2] = {nullptr, nullptr};
+  int cur = 0;
+  int fused = 1;
+  // graphs of one time step, one per starting buffer parity (fused path)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt[2] = {0.0, 0.0};
+  int graph_fused[2] = {-1, -1};
 };
 
 namespace {
@@ -71,55 +76,82 @@ int upload(T **dst, const T *src, size_t n, cudaStream_t s) {
 
 void free_all(wadg_app *a) {
   double *bufs[] = {a->vgeo, a->vfgeo, a->fgeo, a->Jq, a->nrJ, a->nsJ, a->ntJ, a->Drq, a->Dsq,
-                    a->Dtq, a->Drstq, a->VqLq, a->VqPq, a->VfPq, a->Q, a->rhsQ, a->Qf, a->resQ,
-                    a->rhsQf};
+                    a->Dtq, a->Drstq, a->VqLq, a->VqPq, a->VfPq, a->Q, a->uq[0], a->uq[1],
+                    a->uf[0], a->uf[1], a->resQ, a->rhsQf};
   for (double *b : bufs)
     if (b) cudaFree(b);
   if (a->mapPq) cudaFree(a->mapPq);
-  if (a->graph) cudaGraphExecDestroy(a->graph);
+  for (auto &g : a->graph)
+    if (g) cudaGraphExecDestroy(g);
   if (a->ctx) wadg_ctx_destroy(a->ctx);
   if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
 }
 
-int stage(wadg_app *a, double rka, double rkb, double dt) {
+// the three reference kernels on the current buffers (rk_step, euler.c:3610)
+int stage3(wadg_app *a, double rka, double rkb, double dt) {
   int r;
   const int K = a->K;
+  double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
   if (a->p.dim == 3) {
     r = a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
                                              a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq,
-                                             a->Q, a->Qf, a->rhsQ, a->rhsQf)
+                                             a->Q, Qf, rhsQ, a->rhsQf)
                   : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ, a->Drq,
-                                      a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q, a->Qf,
-                                      a->rhsQ, a->rhsQf);
+                                      a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q, Qf,
+                                      rhsQ, a->rhsQf);
     if (r) return r;
-    r = wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf, a->rhsQf, a->rhsQ);
+    r = wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf, a->rhsQf, rhsQ);
     if (r) return r;
     r = a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                                a->rhsQ, a->resQ, a->Q, a->Qf)
-                  : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, a->rhsQ,
-                                         a->resQ, a->Q, a->Qf);
+                                                rhsQ, a->resQ, a->Q, Qf)
+                  : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, rhsQ,
+                                         a->resQ, a->Q, Qf);
   } else {
     r = a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
-                                             a->Dsq, a->VqLq, a->VfPq, a->Q, a->Qf, a->rhsQ,
+                                             a->Dsq, a->VqLq, a->VfPq, a->Q, Qf, rhsQ,
                                              a->rhsQf)
                   : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq, a->Dsq,
-                                      a->VqLq, a->VfPq, a->Q, a->Qf, a->rhsQ, a->rhsQf);
+                                      a->VqLq, a->VfPq, a->Q, Qf, rhsQ, a->rhsQf);
     if (r) return r;
-    r = wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf, a->rhsQf, a->rhsQ);
+    r = wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf, a->rhsQf, rhsQ);
     if (r) return r;
     r = a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                                a->rhsQ, a->resQ, a->Q, a->Qf)
-                  : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, a->rhsQ,
-                                         a->resQ, a->Q, a->Qf);
+                                                rhsQ, a->resQ, a->Q, Qf)
+                  : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, rhsQ,
+                                         a->resQ, a->Q, Qf);
   }
   return r;
 }
 
+// one fused stage: reads buffer cur, writes the other, then flips cur
+int stage_fused(wadg_app *a, double rka, double rkb, double dt) {
+  const int c = a->cur, n = 1 - c;
+  int r = a->p.dim == 3
+              ? wadg_euler_stage_3d(a->ctx, a->K, a->curved, a->vgeo, a->vfgeo, a->fgeo, a->mapPq,
+                                    a->nrJ, a->nsJ, a->ntJ, a->Drq, a->Dsq, a->Dtq, a->VqLq,
+                                    a->VfPq, a->VqPq, a->Jq, rka, rkb, dt, a->uq[c], a->uf[c],
+                                    a->Q, a->resQ, a->uq[n], a->uf[n])
+              : wadg_euler_stage_2d(a->ctx, a->K, a->curved, a->vgeo, a->vfgeo, a->fgeo, a->mapPq,
+                                    a->nrJ, a->nsJ, a->Drq, a->Dsq, a->VqLq, a->VfPq, a->VqPq,
+                                    a->Jq, rka, rkb, dt, a->uq[c], a->uf[c], a->Q, a->resQ,
+                                    a->uq[n], a->uf[n]);
+  if (!r) a->cur = n;
+  return r;
+}
+
+int stage(wadg_app *a, double rka, double rkb, double dt) {
+  return a->fused ? stage_fused(a, rka, rkb, dt) : stage3(a, rka, rkb, dt);
+}
+
+// capture one time step (5 stages) starting from buffer parity a->cur; the
+// fused path flips the parity once per stage, so a step starting at parity p
+// ends at 1-p and two graphs alternate
 int capture_step(wadg_app *a, double dt) {
-  if (a->graph && a->graph_dt == dt) return WADG_OK;
-  if (a->graph) {
-    cudaGraphExecDestroy(a->graph);
-    a->graph = nullptr;
+  const int p = a->cur;
+  if (a->graph[p] && a->graph_dt[p] == dt && a->graph_fused[p] == a->fused) return WADG_OK;
+  if (a->graph[p]) {
+    cudaGraphExecDestroy(a->graph[p]);
+    a->graph[p] = nullptr;
   }
   cudaGraph_t g;
   cudaError_t e = cudaStreamBeginCapture(a->stream, cudaStreamCaptureModeThreadLocal);
@@ -127,12 +159,14 @@ int capture_step(wadg_app *a, double dt) {
   int r = WADG_OK;
   for (int s = 0; s < 5 && r == WADG_OK; ++s) r = stage(a, RK4A[s], RK4B[s], dt);
   e = cudaStreamEndCapture(a->stream, &g);
+  a->cur = p;  // capture does not execute: restore the parity
   if (r) return r;
   if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaStreamEndCapture", e);
-  e = cudaGraphInstantiate(&a->graph, g, 0);
+  e = cudaGraphInstantiate(&a->graph[p], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaGraphInstantiate", e);
-  a->graph_dt = dt;
+  a->graph_dt[p] = dt;
+  a->graph_fused[p] = a->fused;
   return WADG_OK;
 }
 
@@ -208,9 +242,11 @@ int wadg_app_create(const wadg_params *p, int K, int curved, const wadg_host_dat
       (r = upload(&a->VqPq, h->VqPq, Nq * Nq, s)) ||
       (r = upload(&a->VfPq, h->VfPq, NfqNf * Nq, s)) ||
       (r = upload(&a->Q, (const double *)nullptr, K * Nq * Nf, s)) ||
-      (r = upload(&a->rhsQ, (const double *)nullptr, K * Nq * Nf, s)) ||
+      (r = upload(&a->uq[0], (const double *)nullptr, K * Nq * Nf, s)) ||
+      (r = upload(&a->uq[1], (const double *)nullptr, K * Nq * Nf, s)) ||
+      (r = upload(&a->uf[1], (const double *)nullptr, K * NfqNf * Nf, s)) ||
       (r = upload(&a->resQ, (const double *)nullptr, K * Nq * Nf, s)) ||
-      (r = upload(&a->Qf, (const double *)nullptr, K * NfqNf * Nf, s)) ||
+      (r = upload(&a->uf[0], (const double *)nullptr, K * NfqNf * Nf, s)) ||
       (r = upload(&a->rhsQf, (const double *)nullptr, K * NfqNf * Nf, s))) {
     free_all(a);
     delete a;
@@ -243,7 +279,7 @@ int wadg_app_set_state(wadg_app *a, const double *Q, const double *rhsQ, const d
     double *d;
     const double *h;
     size_t n;
-  } c[] = {{a->Q, Q, nv}, {a->rhsQ, rhsQ, nv}, {a->Qf, Qf, nf}, {a->resQ, resQ, nv}};
+  } c[] = {{a->Q, Q, nv}, {a->uq[a->cur], rhsQ, nv}, {a->uf[a->cur], Qf, nf}, {a->resQ, resQ, nv}};
   for (auto &x : c)
     if (x.h) {
       cudaError_t e = cudaMemcpyAsync(x.d, x.h, x.n, cudaMemcpyHostToDevice, a->stream);
@@ -260,7 +296,7 @@ int wadg_app_get_state(wadg_app *a, double *Q, double *rhsQ, double *Qf, double 
     double *h;
     const double *d;
     size_t n;
-  } c[] = {{Q, a->Q, nv}, {rhsQ, a->rhsQ, nv}, {Qf, a->Qf, nf}, {resQ, a->resQ, nv}};
+  } c[] = {{Q, a->Q, nv}, {rhsQ, a->uq[a->cur], nv}, {Qf, a->uf[a->cur], nf}, {resQ, a->resQ, nv}};
   for (auto &x : c)
     if (x.h) {
       cudaError_t e = cudaMemcpyAsync(x.h, x.d, x.n, cudaMemcpyDeviceToHost, a->stream);
@@ -279,11 +315,13 @@ int wadg_rk_step(wadg_app *a, double rka, double rkb, double dt) {
 int wadg_rk_run(wadg_app *a, double dt, int nsteps, int use_graph) {
   if (!a || nsteps < 0) return afail(WADG_ERR_INVALID, "invalid argument");
   if (use_graph) {
-    int r = capture_step(a, dt);
-    if (r) return r;
     for (int t = 0; t < nsteps; ++t) {
-      cudaError_t e = cudaGraphLaunch(a->graph, a->stream);
+      const int p = a->cur;
+      int r = capture_step(a, dt);
+      if (r) return r;
+      cudaError_t e = cudaGraphLaunch(a->graph[p], a->stream);
       if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaGraphLaunch", e);
+      if (a->fused) a->cur = 1 - p;  // 5 stages flip the parity once
     }
     return WADG_OK;
   }
@@ -292,6 +330,12 @@ int wadg_rk_run(wadg_app *a, double dt, int nsteps, int use_graph) {
       int r = stage(a, RK4A[s], RK4B[s], dt);
       if (r) return r;
     }
+  return WADG_OK;
+}
+
+int wadg_app_set_fused(wadg_app *a, int fused) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  a->fused = fused ? 1 : 0;
   return WADG_OK;
 }
 
@@ -321,8 +365,8 @@ int wadg_app_state_ptrs(wadg_app *a, double **Q, double **rhsQ, double **Qf, dou
                         double **rhsQf) {
   if (!a) return afail(WADG_ERR_INVALID, "null app");
   if (Q) *Q = a->Q;
-  if (rhsQ) *rhsQ = a->rhsQ;
-  if (Qf) *Qf = a->Qf;
+  if (rhsQ) *rhsQ = a->uq[a->cur];
+  if (Qf) *Qf = a->uf[a->cur];
   if (resQ) *resQ = a->resQ;
   if (rhsQf) *rhsQf = a->rhsQf;
   return WADG_OK;
@@ -330,9 +374,15 @@ int wadg_app_state_ptrs(wadg_app *a, double **Q, double **rhsQ, double **Qf, dou
 
 int wadg_app_time_run(wadg_app *a, double dt, int nsteps, int use_graph, float *ms) {
   if (!a || !ms) return afail(WADG_ERR_INVALID, "invalid argument");
-  if (use_graph) {
+  if (use_graph) {  // instantiate both parities' graphs outside the timed region
     int r = capture_step(a, dt);
     if (r) return r;
+    if (a->fused) {
+      a->cur = 1 - a->cur;
+      r = capture_step(a, dt);
+      a->cur = 1 - a->cur;
+      if (r) return r;
+    }
   }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -352,6 +402,7 @@ int wadg_app_time_run(wadg_app *a, double dt, int nsteps, int use_graph, float *
 int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
   if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
   const int K = a->K;
+  double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
   cudaEvent_t ev[4];
   for (auto &x : ev) cudaEventCreate(&x);
   float tot[3] = {0, 0, 0};
@@ -362,34 +413,34 @@ int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
     if (a->p.dim == 3)
       r = a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
                                                a->ntJ, a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq,
-                                               a->VfPq, a->Q, a->Qf, a->rhsQ, a->rhsQf)
+                                               a->VfPq, a->Q, Qf, rhsQ, a->rhsQf)
                     : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
                                         a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q,
-                                        a->Qf, a->rhsQ, a->rhsQf);
+                                        Qf, rhsQ, a->rhsQf);
     else
       r = a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
-                                               a->Drq, a->Dsq, a->VqLq, a->VfPq, a->Q, a->Qf,
-                                               a->rhsQ, a->rhsQf)
+                                               a->Drq, a->Dsq, a->VqLq, a->VfPq, a->Q, Qf,
+                                               rhsQ, a->rhsQf)
                     : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
-                                        a->Dsq, a->VqLq, a->VfPq, a->Q, a->Qf, a->rhsQ, a->rhsQf);
+                                        a->Dsq, a->VqLq, a->VfPq, a->Q, Qf, rhsQ, a->rhsQf);
     cudaEventRecord(ev[1], a->stream);
     if (!r)
-      r = a->p.dim == 3 ? wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf,
-                                             a->rhsQf, a->rhsQ)
-                        : wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, a->Qf,
-                                             a->rhsQf, a->rhsQ);
+      r = a->p.dim == 3 ? wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf,
+                                             a->rhsQf, rhsQ)
+                        : wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf,
+                                             a->rhsQf, rhsQ);
     cudaEventRecord(ev[2], a->stream);
     if (!r) {
       if (a->p.dim == 3)
         r = a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
-                                                    dt, a->rhsQ, a->resQ, a->Q, a->Qf)
+                                                    dt, rhsQ, a->resQ, a->Q, Qf)
                       : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                             a->rhsQ, a->resQ, a->Q, a->Qf);
+                                             rhsQ, a->resQ, a->Q, Qf);
       else
         r = a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
-                                                    dt, a->rhsQ, a->resQ, a->Q, a->Qf)
+                                                    dt, rhsQ, a->resQ, a->Q, Qf)
                       : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                             a->rhsQ, a->resQ, a->Q, a->Qf);
+                                             rhsQ, a->resQ, a->Q, Qf);
     }
     cudaEventRecord(ev[3], a->stream);
     cudaError_t e = cudaEventSynchronize(ev[3]);
@@ -404,6 +455,27 @@ int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
   for (auto &x : ev) cudaEventDestroy(x);
   if (r) return r;
   for (int q = 0; q < 3; ++q) ms[q] = tot[q];
+  return WADG_OK;
+}
+
+int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {
+  if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  const int fused = a->fused;
+  a->fused = 1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, a->stream);
+  int r = WADG_OK;
+  for (int s = 0; s < nstages && r == WADG_OK; ++s) r = stage_fused(a, RK4A[s % 5], RK4B[s % 5], dt);
+  cudaEventRecord(e1, a->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  if (!r && e == cudaSuccess) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  a->fused = fused;
+  if (r) return r;
+  if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "time_stage", e);
   return WADG_OK;
 }
 

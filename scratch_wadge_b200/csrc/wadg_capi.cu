@@ -114,6 +114,31 @@ int launch_vol_pairs(const wadg_ctx *c, int K, const double *vgeo, const double 
   return after_launch("volume kernel");
 }
 
+template <int DIM, int N, bool CURVED>
+int launch_stage(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                 const double *fgeo, const uint32_t *mapPq, const double *nrJ, const double *nsJ,
+                 const double *ntJ, const double *Drq, const double *Dsq, const double *Dtq,
+                 const double *VqLq, const double *VfPq, const double *VqPq, const double *Jq,
+                 double fa, double fb, double fdt, const double *uq, const double *uf, double *Q,
+                 double *resQ, double *uq_out, double *uf_out) {
+  constexpr int W = volpairsW<DIM, N, CURVED>();
+  using C = VolPairsCfg<DIM, N, CURVED, W>;
+  auto kern = stage_kernel<DIM, N, CURVED, W>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    if (e != cudaSuccess) return cuda_check(e, "stage kernel smem attribute");
+    attr = true;
+  }
+  const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
+  const int batches = (K + C::E - 1) / C::E;
+  const int grid = batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
+  kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq,
+                                                  Dsq, Dtq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, uq,
+                                                  uf, Q, resQ, uq_out, uf_out, c->phys);
+  return after_launch("stage kernel");
+}
+
 template <int DIM, int N>
 int launch_surf(const wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
                 const double *VqLq, const double *Qf, const double *rhsQf, double *rhsQ) {
@@ -247,6 +272,8 @@ int wadg_ctx_create(const wadg_params *p, wadg_ctx **out) {
   c->phys.gm1 = p->gamma - 1.0;
   c->phys.cbeta = 1.0 / (2.0 * (p->gamma - 1.0));
   c->phys.tau = p->tau;
+  c->phys.lgm1 = log(p->gamma - 1.0);
+  c->phys.igm1 = 1.0 / (p->gamma - 1.0);
   c->stream = (cudaStream_t)p->stream;
   *out = c;
   return WADG_OK;
@@ -379,6 +406,57 @@ int wadg_euler_update_2d_curved(wadg_ctx *c, int K, const double *Jq, const doub
     return fail(WADG_ERR_INVALID, "null pointer argument");
   WADG_DISPATCH(c, return (launch_update<D_, N_, true>(c, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ,
                                                         resQ, Q, Qf)));
+}
+
+// ------------------------------------------------------------ fused stage
+int wadg_euler_stage_3d(wadg_ctx *c, int K, int curved, const double *vgeo, const double *vfgeo,
+                        const double *fgeo, const uint32_t *mapPq, const double *nrJ,
+                        const double *nsJ, const double *ntJ, const double *Drq, const double *Dsq,
+                        const double *Dtq, const double *VqLq, const double *VfPq,
+                        const double *VqPq, const double *Jq, double fa, double fb, double fdt,
+                        const double *rhsQ_in, const double *Qf_in, double *Q, double *resQ,
+                        double *rhsQ_out, double *Qf_out) {
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq, rhsQ_in,
+                Qf_in, Q, resQ, rhsQ_out, Qf_out}) || (curved && !vfgeo))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  if (rhsQ_in == rhsQ_out || Qf_in == Qf_out)
+    return fail(WADG_ERR_INVALID, "stage output buffers must not alias the inputs");
+  if (curved)
+    WADG_DISPATCH(c, return (launch_stage<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                         ntJ, Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq,
+                                                         fa, fb, fdt, rhsQ_in, Qf_in, Q, resQ,
+                                                         rhsQ_out, Qf_out)));
+  WADG_DISPATCH(c, return (launch_stage<D_, N_, false>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                        ntJ, Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq,
+                                                        fa, fb, fdt, rhsQ_in, Qf_in, Q, resQ,
+                                                        rhsQ_out, Qf_out)));
+}
+
+int wadg_euler_stage_2d(wadg_ctx *c, int K, int curved, const double *vgeo, const double *vfgeo,
+                        const double *fgeo, const uint32_t *mapPq, const double *nrJ,
+                        const double *nsJ, const double *Drq, const double *Dsq,
+                        const double *VqLq, const double *VfPq, const double *VqPq,
+                        const double *Jq, double fa, double fb, double fdt,
+                        const double *rhsQ_in, const double *Qf_in, double *Q, double *resQ,
+                        double *rhsQ_out, double *Qf_out) {
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, fgeo, mapPq, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, VqPq, Jq, rhsQ_in, Qf_in, Q,
+                resQ, rhsQ_out, Qf_out}) || (curved && !vfgeo))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  if (rhsQ_in == rhsQ_out || Qf_in == Qf_out)
+    return fail(WADG_ERR_INVALID, "stage output buffers must not alias the inputs");
+  if (curved)
+    WADG_DISPATCH(c, return (launch_stage<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                         nullptr, Drq, Dsq, nullptr, VqLq, VfPq,
+                                                         VqPq, Jq, fa, fb, fdt, rhsQ_in, Qf_in, Q,
+                                                         resQ, rhsQ_out, Qf_out)));
+  WADG_DISPATCH(c, return (launch_stage<D_, N_, false>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                        nullptr, Drq, Dsq, nullptr, VqLq, VfPq,
+                                                        VqPq, Jq, fa, fb, fdt, rhsQ_in, Qf_in, Q,
+                                                        resQ, rhsQ_out, Qf_out)));
 }
 
 }  // extern "C"

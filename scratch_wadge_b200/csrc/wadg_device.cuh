@@ -38,6 +38,8 @@ struct Phys {
   double gm1;     // gamma - 1
   double cbeta;   // 1 / (2 (gamma - 1))
   double tau;     // LF penalty scale of the surface kernel
+  double lgm1;    // log(gamma - 1)
+  double igm1;    // 1 / (gamma - 1)
 };
 
 // 1/x: Newton-Raphson refinement (two steps, quadratic convergence) of the
@@ -179,7 +181,8 @@ __device__ __forceinline__ void VU(const double *U, double *V, const Phys &P) {
 #pragma unroll
   for (int d = 0; d < DIM; ++d) m2 = fma(U[1 + d], U[1 + d], m2);
   const double rhoe = E - 0.5 * m2 / rho;
-  const double s = log(P.gm1 * rhoe / pow(rho, P.gamma));
+  // s = log((gamma-1) rhoe / rho^gamma), written with two logarithms
+  const double s = log(P.gm1 * rhoe) - P.gamma * log(rho);
   const double irhoe = 1.0 / rhoe;
   V[0] = (-E + rhoe * (P.gamma + 1.0 - s)) * irhoe;
 #pragma unroll
@@ -195,7 +198,9 @@ __device__ __forceinline__ void UV(const double *V, double *U, const Phys &P) {
 #pragma unroll
   for (int d = 0; d < DIM; ++d) vv = fma(V[1 + d], V[1 + d], vv);
   const double sV = P.gamma - V[0] + vv / (2.0 * Vl);
-  const double rhoe = pow(P.gm1 / pow(-Vl, P.gamma), 1.0 / P.gm1) * exp(-sV / P.gm1);
+  // rhoe = ((gamma-1)/(-V_l)^gamma)^(1/(gamma-1)) exp(-sV/(gamma-1)), as one
+  // exponential: exp((log(gamma-1) - gamma log(-V_l) - sV) / (gamma-1))
+  const double rhoe = exp((P.lgm1 - P.gamma * log(-Vl) - sV) * P.igm1);
   U[0] = -rhoe * Vl;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) U[1 + d] = rhoe * V[1 + d];

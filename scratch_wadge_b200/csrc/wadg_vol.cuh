@@ -1,4 +1,5 @@
-// Volume flux-differencing kernel, pair-scheduled (the default volume kernel).
+// Pair-scheduled volume kernel (the default volume kernel) and the fused
+// stage kernel built on it.
 //
 // Same mathematics as vol_kernel (wadg_kernels.cuh), organised so that every
 // volume-face pair (i, f) is evaluated once: F_S(u_i, uf_f).nJ_f feeds both
@@ -50,7 +51,10 @@ struct VolPairsCfg {
   static constexpr int pad4of8(int x) { return ((x + 3) / 8) * 8 + 4; }   // == 4 mod 8
   static constexpr int pad2of4(int x) { return ((x + 1) / 4) * 4 + 2; }   // == 2 mod 4
   static constexpr int NGS = CURVED ? El::Nvgeo : 0;  // geometric factors per node
-  static constexpr int SE = pad4of8((El::NS + NGS) * El::NN);
+  static constexpr int mx(int a, int b) { return a > b ? a : b; }
+  // the state block of an element is reused after the pair phase for the row
+  // buffer and the update's staging arrays (3 x Nfields x Nq)
+  static constexpr int SE = pad4of8(mx((El::NS + NGS) * El::NN, 3 * El::Nfields * El::Nq));
   static constexpr int SA = pad2of4(El::Nfields * El::NfqNf);
   static constexpr int SN = El::Nfaces * DIM + El::Nvgeo;
   static constexpr int nD = DIM * El::Nq * El::Nq;
@@ -58,68 +62,70 @@ struct VolPairsCfg {
   static constexpr size_t fixed = sizeof(double) * (size_t)(nD + 2 * nW + El::Nfaces * DIM);
   static constexpr size_t per_elem = sizeof(double) * (size_t)(SE + H * SA + SN);
   static constexpr size_t smem = fixed + E * per_elem;
-  static_assert(SE >= El::Nfields * El::Nq, "row buffer reuses the state region");
 };
 
+// Shared-memory carve-up and the two phases common to both kernels.
 template <int DIM, int N, bool CURVED, int W>
-__global__ void __launch_bounds__(32 * W, 1)
-vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
-                 const double *__restrict__ nrJ, const double *__restrict__ nsJ,
-                 const double *__restrict__ ntJ, const double *__restrict__ Drq,
-                 const double *__restrict__ Dsq, const double *__restrict__ Dtq,
-                 const double *__restrict__ VqLq, const double *__restrict__ VfPq,
-                 const double *__restrict__ Qf, double *__restrict__ rhsQ,
-                 double *__restrict__ rhsQf, Phys P) {
+struct VolPairs {
   using El = Elem<DIM, N>;
   using T = VolTile<DIM, N>;
   using C = VolPairsCfg<DIM, N, CURVED, W>;
-  constexpr int Nq = El::Nq, NF = El::NfqNf, Nfq = El::Nfq, NN = El::NN, NS = El::NS;
-  constexpr int Nf = El::Nfields, NG = El::Nvgeo, L = T::L, R = T::R, G = T::G, E = C::E;
-  constexpr int SE = C::SE, SA = C::SA, SN = C::SN, H = C::H;
+  static constexpr int Nq = El::Nq, NF = El::NfqNf, Nfq = El::Nfq, NN = El::NN, NS = El::NS;
+  static constexpr int Nf = El::Nfields, NG = El::Nvgeo, L = T::L, R = T::R, G = T::G, E = C::E;
+  static constexpr int SE = C::SE, SA = C::SA, SN = C::SN, H = C::H;
 
-  extern __shared__ double smem[];
-  double *sD = smem;                       // Drq | Dsq | Dtq, column-major
-  double *sW1 = sD + C::nD;                // [R][NF][L]  1/2 VqLq(i, f), 0 on padding rows
-  double *sW2 = sW1 + C::nW;               // [R][NF][L] -1/2 VfPq(f, i), 0 on padding rows
-  double *sNr = sW2 + C::nW;               // reference normals [Nfaces][DIM]
-  double *sSt = sNr + El::Nfaces * DIM;    // [E][SE]      node states (+ geometric factors)
-  double *sAcc = sSt + E * SE;             // [E][H][SA]   face-row accumulators, one per warp
-  double *sNrm = sAcc + E * H * SA;        // [E][SN]      per-face nJ (affine) + G
+  double *sD, *sW1, *sW2, *sNr, *sSt, *sAcc, *sNrm;
+  int tid, h, g, l, e;
 
-  const int tid = threadIdx.x;
-  for (int t = tid; t < Nq * Nq; t += blockDim.x) {
-    sD[t] = Drq[t];
-    sD[Nq * Nq + t] = Dsq[t];
-    if (DIM == 3) sD[2 * Nq * Nq + t] = Dtq[t];
-  }
-  for (int t = tid; t < C::nW; t += blockDim.x) {
-    const int l = t % L, s = (t / L) % NF, r = t / (L * NF);
-    const int i = l + L * r;
-    int f = l + s;
-    if (f >= NF) f -= NF;
-    sW1[t] = i < Nq ? 0.5 * VqLq[i + f * Nq] : 0.0;
-    sW2[t] = i < Nq ? -0.5 * VfPq[f + i * NF] : 0.0;
-  }
-  for (int t = tid; t < El::Nfaces; t += blockDim.x) {
-    sNr[t * DIM + 0] = nrJ[t * Nfq];
-    sNr[t * DIM + 1] = nsJ[t * Nfq];
-    if (DIM == 3) sNr[t * DIM + 2] = ntJ[t * Nfq];
+  __device__ __forceinline__ VolPairs(double *smem) {
+    sD = smem;                     // Drq | Dsq | Dtq, column-major
+    sW1 = sD + C::nD;              // [R][NF][L]  1/2 VqLq(i, f), 0 on padding rows
+    sW2 = sW1 + C::nW;             // [R][NF][L] -1/2 VfPq(f, i), 0 on padding rows
+    sNr = sW2 + C::nW;             // reference normals [Nfaces][DIM]
+    sSt = sNr + El::Nfaces * DIM;  // [E][SE]     node states (+ geometric factors)
+    sAcc = sSt + E * SE;           // [E][H][SA]  face-row accumulators, one per warp
+    sNrm = sAcc + E * H * SA;      // [E][SN]     per-face nJ (affine) + G
+    tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    h = warp % H;
+    g = lane / L;
+    l = lane % L;
+    e = (warp / H) * G + g;
   }
 
-  const int warp = tid >> 5, lane = tid & 31;
-  const int h = warp % H;
-  const int g = lane / L, l = lane % L;
-  const int e = (warp / H) * G + g;
+  __device__ __forceinline__ void load_tables(const double *nrJ, const double *nsJ,
+                                              const double *ntJ, const double *Drq,
+                                              const double *Dsq, const double *Dtq,
+                                              const double *VqLq, const double *VfPq) {
+    for (int t = tid; t < Nq * Nq; t += blockDim.x) {
+      sD[t] = Drq[t];
+      sD[Nq * Nq + t] = Dsq[t];
+      if (DIM == 3) sD[2 * Nq * Nq + t] = Dtq[t];
+    }
+    for (int t = tid; t < C::nW; t += blockDim.x) {
+      const int ll = t % L, s = (t / L) % NF, r = t / (L * NF);
+      const int i = ll + L * r;
+      int f = ll + s;
+      if (f >= NF) f -= NF;
+      sW1[t] = i < Nq ? 0.5 * VqLq[i + f * Nq] : 0.0;
+      sW2[t] = i < Nq ? -0.5 * VfPq[f + i * NF] : 0.0;
+    }
+    for (int t = tid; t < El::Nfaces; t += blockDim.x) {
+      sNr[t * DIM + 0] = nrJ[t * Nfq];
+      sNr[t * DIM + 1] = nsJ[t * Nfq];
+      if (DIM == 3) sNr[t * DIM + 2] = ntJ[t * Nfq];
+    }
+  }
 
-  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
-    __syncthreads();  // tables ready / previous batch done with shared memory
-    // ---- node states of the batch (one thread per node); elements past the
-    // end replicate the last element so that every lane computes on valid data
+  // node states of the batch (one thread per node); elements past the end
+  // replicate the last element so that every lane computes on valid data
+  __device__ __forceinline__ void prologue(int K, int k0, const double *vgeo, const double *vfgeo,
+                                           const double *uq, const double *uf, const Phys &P) {
     for (int t = tid; t < E * NN; t += blockDim.x) {
       const int ee = t / NN, n = t % NN;
       const int k = min(k0 + ee, K - 1);
-      const NodeState<DIM> s = (n < Nq) ? node_state<DIM>(rhsQ + (size_t)k * Nq * Nf + n, Nq, P)
-                                        : node_state<DIM>(Qf + (size_t)k * NF * Nf + (n - Nq), NF, P);
+      const NodeState<DIM> s = (n < Nq) ? node_state<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
+                                        : node_state<DIM>(uf + (size_t)k * NF * Nf + (n - Nq), NF, P);
       double *st = sSt + ee * SE;
       st[0 * NN + n] = s.rho;
 #pragma unroll
@@ -154,30 +160,31 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           }
       }
     }
-    __syncthreads();
+  }
 
-    const int k = k0 + e;
-    const bool kval = k < K;
-    double *st = sSt + e * SE;
-    double *acc_f = sAcc + (e * H + h) * SA;
-    auto load = [&](int n) {
-      NodeState<DIM> s;
-      s.rho = st[n];
+  __device__ __forceinline__ NodeState<DIM> load(const double *st, int n) const {
+    NodeState<DIM> s;
+    s.rho = st[n];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) s.vel[d] = st[(1 + d) * NN + n];
-      s.beta = st[(DIM + 1) * NN + n];
-      s.lrho = st[(DIM + 2) * NN + n];
-      s.lbeta = st[(DIM + 3) * NN + n];
-      return s;
-    };
+    for (int d = 0; d < DIM; ++d) s.vel[d] = st[(1 + d) * NN + n];
+    s.beta = st[(DIM + 1) * NN + n];
+    s.lrho = st[(DIM + 2) * NN + n];
+    s.lbeta = st[(DIM + 3) * NN + n];
+    return s;
+  }
 
+  // all flux pairs of element e: this warp's half of the volume columns and of
+  // the face steps; rows into acc (registers), face rows into this warp's
+  // accumulator copy
+  __device__ __forceinline__ void pairs(double (&acc)[R][Nf], const Phys &P) const {
+    const double *st = sSt + e * SE;
+    double *acc_f = sAcc + (e * H + h) * SA;
     NodeState<DIM> A[R];
     int ir[R];
-    double acc[R][Nf];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       ir[r] = min(l + L * r, Nq - 1);  // padding row computes on a clamped index
-      A[r] = load(ir[r]);
+      A[r] = load(st, ir[r]);
 #pragma unroll
       for (int q = 0; q < Nf; ++q) acc[r][q] = 0.0;
     }
@@ -187,10 +194,10 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
       for (int c = 0; c < NG; ++c) Ge[c] = sNrm[e * SN + El::Nfaces * DIM + c];
     }
 
-    // ---- volume-volume pairs: warp h takes columns [j0, j1)
+    // volume-volume pairs: warp h takes columns [j0, j1)
     const int j0 = h ? Nq / 2 : 0, j1 = h ? Nq : Nq / 2;
     for (int j = j0; j < j1; ++j) {
-      const NodeState<DIM> B = load(j);
+      const NodeState<DIM> B = load(st, j);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int i = ir[r];
@@ -214,12 +221,12 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
       }
     }
 
-    // ---- volume-face pairs, each evaluated once: warp h takes steps [s0, s1)
+    // volume-face pairs, each evaluated once: warp h takes steps [s0, s1)
     const int s0 = h ? NF / 2 : 0, s1 = h ? NF : NF / 2;
     for (int s = s0; s < s1; ++s) {
       int f = l + s;
       if (f >= NF) f -= NF;
-      const NodeState<DIM> B = load(Nq + f);
+      const NodeState<DIM> B = load(st, Nq + f);
       const int fc = f / Nfq;
       double nv[DIM];
       if (!CURVED) {
@@ -257,10 +264,12 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
       for (int q = 0; q < Nf; ++q) acc_f[q * NF + f] += af[q];
       __syncwarp();
     }
+  }
 
-    // ---- combine the two warps' partial rows; write rows and face rows
-    __syncthreads();  // all pairs done: the state region becomes the row buffer
-    double *rowbuf = st;  // [Nf][Nq] partial rows of warp 1
+  // warp 1 parks its partial rows in element e's state block ([Nf][Nq]);
+  // call between two __syncthreads
+  __device__ __forceinline__ void park_rows(const double (&acc)[R][Nf]) const {
+    double *rowbuf = sSt + e * SE;
     if (h == 1) {
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -271,12 +280,40 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
         }
       }
     }
+  }
+};
+
+template <int DIM, int N, bool CURVED, int W>
+__global__ void __launch_bounds__(32 * W, 1)
+vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
+                 const double *__restrict__ nrJ, const double *__restrict__ nsJ,
+                 const double *__restrict__ ntJ, const double *__restrict__ Drq,
+                 const double *__restrict__ Dsq, const double *__restrict__ Dtq,
+                 const double *__restrict__ VqLq, const double *__restrict__ VfPq,
+                 const double *__restrict__ Qf, double *__restrict__ rhsQ,
+                 double *__restrict__ rhsQf, Phys P) {
+  using V = VolPairs<DIM, N, CURVED, W>;
+  constexpr int Nq = V::Nq, NF = V::NF, Nf = V::Nf, R = V::R, L = V::L, E = V::E, H = V::H;
+  extern __shared__ double smem[];
+  V v(smem);
+  v.load_tables(nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq);
+
+  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
+    __syncthreads();  // tables ready / previous batch done with shared memory
+    v.prologue(K, k0, vgeo, vfgeo, rhsQ, Qf, P);
     __syncthreads();
-    if (kval) {
-      if (h == 0) {
+    double acc[R][Nf];
+    v.pairs(acc, P);
+    __syncthreads();  // all pairs done: the state block becomes the row buffer
+    v.park_rows(acc);
+    __syncthreads();
+    const int k = k0 + v.e;
+    if (k < K) {
+      const double *rowbuf = v.sSt + v.e * V::SE;
+      if (v.h == 0) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int i = l + L * r;
+          const int i = v.l + L * r;
           if (i < Nq) {
             double *out = rhsQ + (size_t)k * Nq * Nf + i;
 #pragma unroll
@@ -284,9 +321,218 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           }
         }
       }
-      const double *a0 = sAcc + (e * H + 0) * SA, *a1 = sAcc + (e * H + 1) * SA;
+      const double *a0 = v.sAcc + (v.e * H + 0) * V::SA, *a1 = v.sAcc + (v.e * H + 1) * V::SA;
       double *outf = rhsQf + (size_t)k * NF * Nf;
-      for (int t = h * L + l; t < NF * Nf; t += H * L) outf[t] = a0[t] + a1[t];
+      for (int t = v.h * L + v.l; t < NF * Nf; t += H * L) outf[t] = a0[t] + a1[t];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- fused stage
+// One LSRK stage in one launch: volume pairs, surface flux + LF penalty, lift,
+// inverse mass, LSRK update and entropy projection -- rk_step of the reference
+// (euler.c:3610-3666: euler_vol_3d, euler_surf_3d, euler_update_3d or the
+// curved / 2D counterparts) with the intermediates (rhsQf, the volume RHS)
+// kept in shared memory.  The entropy-projected state is read from (uq, uf)
+// and written to (uq_out, uf_out), distinct buffers, because the surface flux
+// of an element reads its neighbours' traces of the current stage while other
+// CTAs already write the next stage's.  Q and resQ are updated in place (each
+// element touches only its own).
+template <int DIM, int N, bool CURVED, int W>
+__global__ void __launch_bounds__(32 * W, 1)
+stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
+             const double *__restrict__ fgeo, const uint32_t *__restrict__ mapPq,
+             const double *__restrict__ nrJ, const double *__restrict__ nsJ,
+             const double *__restrict__ ntJ, const double *__restrict__ Drq,
+             const double *__restrict__ Dsq, const double *__restrict__ Dtq,
+             const double *__restrict__ VqLq, const double *__restrict__ VfPq,
+             const double *__restrict__ VqPq, const double *__restrict__ Jq, double fa,
+             double fb, double fdt, const double *__restrict__ uq, const double *__restrict__ uf,
+             double *__restrict__ Q, double *__restrict__ resQ, double *__restrict__ uq_out,
+             double *__restrict__ uf_out, Phys P) {
+  using V = VolPairs<DIM, N, CURVED, W>;
+  using El = Elem<DIM, N>;
+  constexpr int Nq = V::Nq, NF = V::NF, Nf = V::Nf, R = V::R, L = V::L, E = V::E, H = V::H;
+  constexpr int SE = V::SE, SA = V::SA, NFG = El::Nfgeo;
+  extern __shared__ double smem[];
+  V v(smem);
+  v.load_tables(nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq);
+  const int tid = threadIdx.x, nth = blockDim.x;
+
+  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
+    __syncthreads();
+    v.prologue(K, k0, vgeo, vfgeo, uq, uf, P);
+    __syncthreads();
+    double acc[R][Nf];
+    v.pairs(acc, P);
+    __syncthreads();
+
+    // ---- surface: sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam) sJ (u+ - u-)
+    // (Euler3D.okl:3256-3346, Euler2D.okl:1373-1453); stored over copy 0 of
+    // the face accumulators
+    for (int t = tid; t < E * NF; t += nth) {
+      const int ee = t / NF, f = t % NF, k = k0 + ee;
+      if (k >= K) continue;
+      const size_t idM = f + (size_t)k * NF * Nf;
+      const size_t idP = mapPq[f + (size_t)k * NF];
+      const double *fg = fgeo + (size_t)k * NF * NFG + f;
+      double nJ[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nJ[d] = fg[d * NF];
+      const double sJ = fg[DIM * NF];
+      double UM[Nf], UP[Nf];
+#pragma unroll
+      for (int q = 0; q < Nf; ++q) {
+        UM[q] = uf[idM + q * NF];
+        UP[q] = uf[idP + q * NF];
+      }
+      const NodeState<DIM> M = v.load(v.sSt + ee * SE, Nq + f);
+      const NodeState<DIM> Pp = node_state<DIM>(UP, 1, P);
+      double F[Nf];
+      ecflux_n<DIM>(M, Pp, nJ, P, F);
+      double kM = 0.0, kP = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const double um = UM[1 + d] / UM[0], up = UP[1 + d] / UP[0];
+        kM = fma(um, um, kM);
+        kP = fma(up, up, kP);
+      }
+      const double pM = P.gm1 * (UM[Nf - 1] - 0.5 * UM[0] * kM);
+      const double pP = P.gm1 * (UP[Nf - 1] - 0.5 * UP[0] * kP);
+      const double lamM = sqrt(kM) + sqrt(P.gamma * pM / UM[0]);
+      const double lamP = sqrt(kP) + sqrt(P.gamma * pP / UP[0]);
+      const double tau = (DIM == 3) ? P.tau : 1.0;
+      const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
+      double *a0 = v.sAcc + (ee * H + 0) * SA;
+      const double *a1 = v.sAcc + (ee * H + 1) * SA;
+#pragma unroll
+      for (int q = 0; q < Nf; ++q)
+        a0[q * NF + f] = (a0[q * NF + f] + a1[q * NF + f]) + 0.5 * F[q] - Lfc * (UP[q] - UM[q]);
+    }
+    __syncthreads();
+
+    // ---- lift: rows += VqLq sfS, on the rotated weights (VqLq = 2 W1),
+    // the two warps splitting the face nodes as in the pair phase
+    {
+      const double *sf = v.sAcc + (v.e * H + 0) * SA;
+      const int s0 = v.h ? NF / 2 : 0, s1 = v.h ? NF : NF / 2;
+      for (int s = s0; s < s1; ++s) {
+        int f = v.l + s;
+        if (f >= NF) f -= NF;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double w = 2.0 * v.sW1[(r * NF + s) * L + v.l];
+#pragma unroll
+          for (int q = 0; q < Nf; ++q) acc[r][q] = fma(w, sf[q * NF + f], acc[r][q]);
+        }
+      }
+    }
+    v.park_rows(acc);  // the state block is free after the surface phase
+    __syncthreads();
+    if (v.h == 0) {
+      double *rowbuf = v.sSt + v.e * SE;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = v.l + L * r;
+        if (i < Nq) {
+#pragma unroll
+          for (int q = 0; q < Nf; ++q) rowbuf[q * Nq + i] += acc[r][q];  // full RHS row
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- update (Euler3Daffine.okl:555-773 / Euler3D.okl:2527-2884):
+    // staging per element in its state block: [0] rhs, [1] sA, [2] sB
+    auto blk = [&](int ee, int which) { return v.sSt + ee * SE + which * Nf * Nq; };
+    auto matvec = [&](const double *Op, int ld, int row, const double *X, double *out) {
+#pragma unroll
+      for (int q = 0; q < Nf; ++q) out[q] = 0.0;
+      for (int j = 0; j < Nq; ++j) {
+        const double w = __ldg(Op + row + j * ld);
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) out[q] = fma(w, X[q * Nq + j], out[q]);
+      }
+    };
+    if (CURVED) {
+      for (int t = tid; t < E * Nq; t += nth) {
+        const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+        if (k >= K) continue;
+        double r[Nf];
+        matvec(VqPq, Nq, i, blk(ee, 0), r);
+        const double Jqi = Jq[(size_t)k * Nq + i];
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) blk(ee, 1)[q * Nq + i] = -2.0 * r[q] / Jqi;
+      }
+      __syncthreads();
+    }
+    for (int t = tid; t < E * Nq; t += nth) {
+      const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+      if (k >= K) continue;
+      const double Jqi = Jq[(size_t)k * Nq + i];
+      double r[Nf], U[Nf], Vv[Nf];
+      if (CURVED) {
+        matvec(VqPq, Nq, i, blk(ee, 1), r);
+      } else {
+        matvec(VqPq, Nq, i, blk(ee, 0), r);
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) r[q] = -2.0 * r[q] / Jqi;
+      }
+      const size_t id = (size_t)k * Nq * Nf + i;
+#pragma unroll
+      for (int q = 0; q < Nf; ++q) {
+        const double res = fa * resQ[id + q * Nq] + fdt * r[q];
+        resQ[id + q * Nq] = res;
+        U[q] = Q[id + q * Nq] + fb * res;
+        Q[id + q * Nq] = U[q];
+      }
+      VU<DIM>(U, Vv, P);
+#pragma unroll
+      for (int q = 0; q < Nf; ++q) blk(ee, 2)[q * Nq + i] = CURVED ? Vv[q] * Jqi : Vv[q];
+    }
+    __syncthreads();
+    int src = 2;  // block holding the projected entropy variables' source
+    if (CURVED) {
+      // weight-adjusted projection VqPq((VqPq (v J)) / J)
+      for (int t = tid; t < E * Nq; t += nth) {
+        const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+        if (k >= K) continue;
+        double r[Nf];
+        matvec(VqPq, Nq, i, blk(ee, 2), r);
+        const double Jqi = Jq[(size_t)k * Nq + i];
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) blk(ee, 1)[q * Nq + i] = r[q] / Jqi;
+      }
+      __syncthreads();
+      for (int t = tid; t < E * Nq; t += nth) {
+        const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+        if (k >= K) continue;
+        double r[Nf];
+        matvec(VqPq, Nq, i, blk(ee, 1), r);
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) blk(ee, 0)[q * Nq + i] = r[q];
+      }
+      __syncthreads();
+      src = 0;
+    }
+    for (int t = tid; t < E * (NF + Nq); t += nth) {
+      const int ee = t / (NF + Nq), n = t % (NF + Nq), k = k0 + ee;
+      if (k >= K) continue;
+      double Vv[Nf], U[Nf];
+      if (n < NF) {
+        matvec(VfPq, NF, n, blk(ee, src), Vv);
+        UV<DIM>(Vv, U, P);
+        double *out = uf_out + (size_t)k * NF * Nf + n;
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) out[q * NF] = U[q];
+      } else {
+        const int i = n - NF;
+        matvec(VqPq, Nq, i, blk(ee, src), Vv);
+        UV<DIM>(Vv, U, P);
+        double *out = uq_out + (size_t)k * Nq * Nf + i;
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) out[q * Nq] = U[q];
+      }
     }
   }
 }

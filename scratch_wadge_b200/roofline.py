@@ -53,3 +53,15 @@ def surf_bytes_per_element(dim, Nq, NfqNf):
 def update_bytes_per_element(dim, Nq, NfqNf):
     Nf = dim + 2
     return 8 * Nf * Nq * 6 + 8 * Nq + 8 * Nf * NfqNf
+
+
+def stage_flops_per_element(dim, Nq, NfqNf, curved, series=True):
+    """Algorithmic flops of the fused stage kernel per element: the volume
+    pairs, the surface flux (one face-volume pair's count per face node), the
+    lift VqLq*sfS and the update's matrix-vector products (2 flops per
+    multiply-add; affine: -2 VqPq rhs, VfPq v, VqPq v; WADG adds two more
+    Nq x Nq products).  VU/UV transcendentals are not counted."""
+    Nf = dim + 2
+    vf = PAIR_FLOPS[(dim, bool(curved), bool(series))][1]
+    mm = 2 * Nf * (Nq * NfqNf + (Nq * Nq * (4 if curved else 2)) + NfqNf * Nq)
+    return vol_flops_per_element(dim, Nq, NfqNf, curved, series) + NfqNf * vf + mm

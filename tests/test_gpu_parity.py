@@ -63,6 +63,16 @@ class Dev:
                         g["VfPq"].data_ptr(), a, b, dt, s["rhsQ"].data_ptr(), s["resQ"].data_ptr(),
                         s["Q"].data_ptr(), s["Qf"].data_ptr())
 
+    def stage(self, s, out, a, b, dt):
+        g = self.g
+        self.ctx.stage(self.curved, self.geo.K, g["vgeo"].data_ptr(), g["vfgeo"].data_ptr(),
+                       g["fgeo"].data_ptr(), g["mapPq"].data_ptr(), g["nrJ"].data_ptr(),
+                       g["nsJ"].data_ptr(), g["ntJ"].data_ptr(), g["Drq"].data_ptr(), g["Dsq"].data_ptr(),
+                       g["Dtq"].data_ptr(), g["VqLq"].data_ptr(), g["VfPq"].data_ptr(),
+                       g["VqPq"].data_ptr(), g["Jq"].data_ptr(), a, b, dt, s["rhsQ"].data_ptr(),
+                       s["Qf"].data_ptr(), s["Q"].data_ptr(), s["resQ"].data_ptr(),
+                       out["rhsQ"].data_ptr(), out["Qf"].data_ptr())
+
     def sync(self):
         self.torch.cuda.synchronize()
 
@@ -110,6 +120,46 @@ def test_stage_matches_oracle_perturbed(cuda, name):
         h = d.get(s)
         for k in ("Q", "rhsQ", "Qf", "resQ"):
             assert rel(h[k], a[k]) < RTOL, (k, rel(h[k], a[k]))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fused_stage_matches_reference_golden(cuda, name):
+    """wadg_euler_stage_*: one launch = vol + surf + update of the reference."""
+    c = Case(name)
+    d = Dev(cuda, c.geo, c.curved)
+    s = d.put(c.state())
+    out = {"rhsQ": cuda.empty_like(s["rhsQ"]), "Qf": cuda.empty_like(s["Qf"])}
+    d.stage(s, out, IC.RK4A[1], IC.RK4B[1], c.dt)
+    d.sync()
+    got = dict(Q=s["Q"].cpu().numpy(), resQ=s["resQ"].cpu().numpy(),
+               rhsQ=out["rhsQ"].cpu().numpy(), Qf=out["Qf"].cpu().numpy())
+    for k in ("Q", "rhsQ", "Qf", "resQ"):
+        assert rel(got[k], c.z["upd_" + k]) < RTOL, (k, rel(got[k], c.z["upd_" + k]))
+    # the inputs are untouched
+    assert np.array_equal(s["rhsQ"].cpu().numpy(), c.z["in_rhsQ"])
+
+
+def test_fused_stage_rejects_aliasing(cuda):
+    c = Case("tg3d_affine_N3")
+    d = Dev(cuda, c.geo, c.curved)
+    s = d.put(c.state())
+    with pytest.raises(capi.WadgError):
+        d.stage(s, {"rhsQ": s["rhsQ"], "Qf": s["Qf"]}, IC.RK4A[1], IC.RK4B[1], c.dt)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fused_and_three_kernel_paths_agree(cuda, name):
+    c = Case(name)
+    outs = []
+    for fused in (True, False):
+        app = capi.App(c.geo, c.curved)
+        app.set_fused(fused)
+        st = c.state()
+        app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
+        app.rk_run(c.dt, 3, graph=True)
+        outs.append(app.get_state())
+    for k in ("Q", "rhsQ", "Qf"):
+        assert rel(outs[0][k], outs[1][k]) < RTOL, k
 
 
 @pytest.mark.parametrize("name", golden_names())
