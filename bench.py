@@ -224,7 +224,21 @@ def run_ours(args):
         barrier()
         app.close()
         return
-    # warm-up (also captures the time-step graph)
+    # warm-up (also captures the time-step graphs) and the choice between the
+    # two stage implementations: three reference kernels or the fused kernel
+    variants = {}
+    for fused in (False, True):
+        app.set_fused(fused)
+        app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
+        app.rk_run(dt, max(args.warmup, 1), graph=True)
+        variants["fused" if fused else "three_kernels"] = app.time_run(dt, 10, graph=True) / 10
+    use_fused = variants["fused"] < variants["three_kernels"]
+    if pg:  # every rank takes the same variant
+        t = torch.tensor([1.0 if use_fused else 0.0], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        use_fused = bool(t.item() > 0)
+    app.set_fused(use_fused)
+    app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     app.rk_run(dt, max(args.warmup, 1), graph=True)
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -306,7 +320,9 @@ def run_ours(args):
                     "step": f"one wadg_app_solve_host call: H2D stage-0 state, {E2E_STEPS} time "
                             f"steps, D2H Q (pinned host buffers, wall clock)",
                     "calls": e2e_calls},
-            "gpu_launches": 5 * args.steps,
+            "gpu_launches": (5 if use_fused else 15) * args.steps,
+            "stage_variant": {"used": "fused" if use_fused else "three_kernels",
+                              "ms_per_step": variants},
             "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))

@@ -207,8 +207,8 @@ int wadg_app_solve_host(wadg_app *app, const double *Q0, const double *rhsQ0,
                         int nsteps, double *Q, double *rhsQ, double *Qf,
                         double *resQ);
 int wadg_app_sync(wadg_app *app);
-/* fused != 0 (the default): wadg_rk_step / wadg_rk_run launch the fused stage
- * kernel (one launch per stage, ping-pong state buffers); 0: the three
+/* fused != 0: wadg_rk_step / wadg_rk_run launch the fused stage kernel (one
+ * launch per stage, ping-pong state buffers); 0 (the default): the three
  * reference kernels per stage.  Results agree to rounding. */
 int wadg_app_set_fused(wadg_app *app, int fused);
 /* device pointers of the state arrays (for zero-copy use and testing) */

@@ -51,7 +51,7 @@ struct wadg_app {
   double *Q = nullptr, *resQ = nullptr, *rhsQf = nullptr;
   double *uq[2] = {nullptr, nullptr}, *uf[2] = {nullptr, nullptr};
   int cur = 0;
-  int fused = 1;
+  int fused = 0;
   // graphs of one time step, one per starting buffer parity (fused path)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double graph_dt[2] = {0.0, 0.0};

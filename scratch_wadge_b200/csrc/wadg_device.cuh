@@ -256,3 +256,55 @@ __device__ __forceinline__ void ecflux_n_warp(const NodeState<DIM> &a, const Nod
 }
 
 }  // namespace wadg
+
+namespace wadg {
+
+// Two-point flux for states without precomputed logarithms (surface traces):
+// the log branch of the log-mean evaluates log(a/b) itself, as the reference
+// does; the series branches are those of logmean / inv_logmean.
+template <int DIM>
+__device__ __forceinline__ void ecflux_n_nolog(const NodeState<DIM> &a, const NodeState<DIM> &b,
+                                               const double *n, const Phys &P, double *F) {
+  const double sr = a.rho + b.rho, dr = a.rho - b.rho;
+  const double sb = a.beta + b.beta, db = a.beta - b.beta;
+  const double isr = rcp(sr), isb = rcp(sb);
+  const double fr = dr * isr, fb = db * isb;
+  const double ur = fr * fr, ub = fb * fb;
+  const double rl = (ur < 1e-2) ? 0.5 * sr * polyG(ur) : dr / log(a.rho / b.rho);
+  const double ibl = (ub < 1e-2) ? 2.0 * isb * polyF(ub) : log(a.beta / b.beta) / db;
+  const double pa = 0.5 * sr * isb;
+  double ub2[DIM], un = 0.0, vv = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    ub2[d] = 0.5 * (a.vel[d] + b.vel[d]);
+    un = fma(ub2[d], n[d], un);
+    vv = fma(a.vel[d], b.vel[d], vv);
+  }
+  const double f4 = fma(rl, fma(ibl, P.cbeta, 0.5 * vv), pa);
+  const double F0 = rl * un;
+  F[0] = F0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = fma(F0, ub2[d], pa * n[d]);
+  F[DIM + 1] = f4 * un;
+}
+
+// node state without the logarithms (for ecflux_n_nolog)
+template <int DIM>
+__device__ __forceinline__ NodeState<DIM> node_state_nolog(const double *q, int stride, const Phys &P) {
+  NodeState<DIM> s;
+  s.rho = q[0];
+  const double ir = 1.0 / s.rho;
+  double kin = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.vel[d] = q[(1 + d) * stride] * ir;
+    kin = fma(s.vel[d], s.vel[d], kin);
+  }
+  const double p = P.gm1 * (q[(DIM + 1) * stride] - 0.5 * s.rho * kin);
+  s.beta = s.rho / (2.0 * p);
+  s.lrho = 0.0;
+  s.lbeta = 0.0;
+  return s;
+}
+
+}  // namespace wadg

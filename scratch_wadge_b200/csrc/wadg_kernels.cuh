@@ -202,10 +202,10 @@ surf_kernel(int K, const double *__restrict__ fgeo, const uint32_t *__restrict__
       UM[f] = Qf[idM + f * NfqNf];
       UP[f] = Qf[idP + f * NfqNf];
     }
-    const NodeState<DIM> M = node_state<DIM>(UM, 1, P);
-    const NodeState<DIM> Pp = node_state<DIM>(UP, 1, P);
+    const NodeState<DIM> M = node_state_nolog<DIM>(UM, 1, P);
+    const NodeState<DIM> Pp = node_state_nolog<DIM>(UP, 1, P);
     double F[Nf];
-    ecflux_n<DIM>(M, Pp, nJ, P, F);
+    ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
     // wave speeds |u| + sqrt(gamma p / rho), p = rho / (2 beta)
     double kM = 0.0, kP = 0.0;
 #pragma unroll
@@ -344,22 +344,25 @@ update_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ V
       for (int f = 0; f < Nf; ++f) sV[e][f][i] = V[f];
   }
   __syncthreads();
-  if (!valid) return;
 
-  for (int ii = i; ii < NfqNf; ii += Nq) {
-    double Vf[Nf], Uf[Nf];
-    matvec(VfPq, NfqNf, ii, X[e], Vf);
-    UV<DIM>(Vf, Uf, P);
-    double *out = Qf + (size_t)k * NfqNf * Nf + ii;
+  // face and volume outputs spread evenly over the CTA's threads
+  for (int t = threadIdx.x; t < kend * (NfqNf + Nq); t += blockDim.x) {
+    const int ee = t / (NfqNf + Nq), n = t % (NfqNf + Nq), kk = k0 + ee;
+    double Vv[Nf], Uu[Nf];
+    if (n < NfqNf) {
+      matvec(VfPq, NfqNf, n, X[ee], Vv);
+      UV<DIM>(Vv, Uu, P);
+      double *out = Qf + (size_t)kk * NfqNf * Nf + n;
 #pragma unroll
-    for (int f = 0; f < Nf; ++f) out[f * NfqNf] = Uf[f];
+      for (int f = 0; f < Nf; ++f) out[f * NfqNf] = Uu[f];
+    } else {
+      matvec(VqPq, Nq, n - NfqNf, X[ee], Vv);
+      UV<DIM>(Vv, Uu, P);
+      double *out = rhsQ + (size_t)kk * Nq * Nf + (n - NfqNf);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) out[f * Nq] = Uu[f];
+    }
   }
-  double Vq[Nf], Uq[Nf];
-  matvec(VqPq, Nq, i, X[e], Vq);
-  UV<DIM>(Vq, Uq, P);
-  double *out = rhsQ + (size_t)k * Nq * Nf + i;
-#pragma unroll
-  for (int f = 0; f < Nf; ++f) out[f * Nq] = Uq[f];
 }
 
 }  // namespace wadg

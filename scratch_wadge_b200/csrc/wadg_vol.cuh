@@ -387,9 +387,9 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
         UP[q] = uf[idP + q * NF];
       }
       const NodeState<DIM> M = v.load(v.sSt + ee * SE, Nq + f);
-      const NodeState<DIM> Pp = node_state<DIM>(UP, 1, P);
+      const NodeState<DIM> Pp = node_state_nolog<DIM>(UP, 1, P);
       double F[Nf];
-      ecflux_n<DIM>(M, Pp, nJ, P, F);
+      ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
       double kM = 0.0, kP = 0.0;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
