@@ -324,6 +324,8 @@ def run_ours(args):
             "stage_variant": {"used": "fused" if use_fused else "three_kernels",
                               "ms_per_step": variants},
             "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks}
+    if not args.no_ensemble:
+        line["ensemble"] = run_ensemble_measurement()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
         sec, kind = time_cpu(geo, st0, dt, 2)
@@ -337,6 +339,44 @@ def run_ours(args):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def run_ensemble_measurement(steps=5, warmup=2):
+    """256 independent 2D vortex solves (K log-uniform in
+    [200, 8192], N uniform in {2,3,4}, seeded), batched (bins + one CUDA graph
+    per time step) against the plain one-instance-per-launch path, same dt and
+    steps; throughput in DOF*stages/s, timed with CUDA events."""
+    from scratch_wadge_b200 import ensemble as EN
+    t0 = time.perf_counter()
+    inst = EN.draw_instances(n=256, kmin=200, kmax=8192, degrees=(2, 3, 4), seed=0)
+    parts = [EN.build_instance(i) for i in inst]
+    dt = EN.common_dt(parts)
+    setup_s = time.perf_counter() - t0
+    out = {"instances": len(inst), "K_total": sum(i.K for i in inst),
+           "degrees": {str(N): sum(1 for i in inst if i.N == N) for N in (2, 3, 4)},
+           "setup_s": setup_s, "steps": steps}
+    res = {}
+    for fused in (False, True):
+        ens = EN.Ensemble(inst, parts, fused=fused)
+        ens.run(dt, warmup)
+        ms = ens.time_run(dt, steps)
+        res["fused" if fused else "three_kernels"] = ms / steps
+        dofs = ens.dofs
+        ens.close()
+    best = min(res.values())
+    single = EN.SingleInstances(inst, parts)
+    single.run(dt, 1)
+    ms_single = single.time_run(dt, max(2, steps // 2)) / max(2, steps // 2)
+    single.close()
+    out.update({"dofs_per_field": dofs,
+                "batched_ms_per_step": best, "batched_variant_ms": res,
+                "batched_value": dofs * 5 / (best * 1e-3),
+                "single_ms_per_step": ms_single,
+                "single_value": dofs * 5 / (ms_single * 1e-3),
+                "speedup": ms_single / best, "unit": UNIT,
+                "single_path": "one wadg_app per instance, 3 kernels x 5 stages launched per instance",
+                "batched_path": "one bin per degree (concatenated instances), one CUDA graph per step, bins on concurrent streams"})
+    return out
 
 
 def fp64_peak(stream):
@@ -362,6 +402,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + steps of the device path (for ncu), no JSON line")
     args = ap.parse_args()

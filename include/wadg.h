@@ -225,6 +225,27 @@ int wadg_app_time_kernels(wadg_app *app, double dt, int nstages, float *ms);
  * ms receives the total. */
 int wadg_app_time_stage(wadg_app *app, double dt, int nstages, float *ms);
 
+/* the app's CUDA stream (a cudaStream_t) */
+void *wadg_app_stream(wadg_app *app);
+/* fused-stage ping-pong: which state buffer is current (0 or 1).  The state
+ * accessors read the current buffer; set only to undo a capture. */
+int wadg_app_set_parity(wadg_app *app, int parity);
+int wadg_app_get_fused(wadg_app *app);
+
+/* ------------------------------------------------------------ ensemble
+ * Batched ensemble of independent solves.  A bin is one wadg_app holding the
+ * concatenation of all instances of one degree (neighbour maps offset per
+ * instance, one common dt); wadg_ensemble_run replays one CUDA graph per time
+ * step whose branches -- one per bin, on the bins' own streams -- run
+ * concurrently.  The reference runs one instance per process; no
+ * counterpart. */
+typedef struct wadg_ensemble wadg_ensemble;
+int wadg_ensemble_create(int nbins, wadg_app **bins, wadg_ensemble **out);
+int wadg_ensemble_destroy(wadg_ensemble *ens);
+int wadg_ensemble_run(wadg_ensemble *ens, double dt, int nsteps);
+int wadg_ensemble_sync(wadg_ensemble *ens);
+int wadg_ensemble_time_run(wadg_ensemble *ens, double dt, int nsteps, float *ms);
+
 /* ------------------------------------------------------------ measurement
  * FP64 FMA throughput of the current GPU (the denominator of the volume
  * kernel's FP64 roofline): a saturating FMA kernel timed with CUDA events on

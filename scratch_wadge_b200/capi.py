@@ -79,6 +79,12 @@ def lib():
         L.wadg_app_time_stage.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
         L.wadg_probe_fp64_fma.argtypes = [v, i, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_float)]
+        L.wadg_app_stream.restype = ctypes.c_void_p
+        L.wadg_app_stream.argtypes = [v]
+        L.wadg_app_set_parity.argtypes = [v, i]
+        L.wadg_app_get_fused.argtypes = [v]
+        L.wadg_ensemble_destroy.argtypes = [v]
+        L.wadg_ensemble_sync.argtypes = [v]
         L.wadg_app_create.argtypes = [ctypes.POINTER(Params), i, i, ctypes.POINTER(HostData),
                                       ctypes.POINTER(ctypes.c_void_p)]
         L.wadg_ctx_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]

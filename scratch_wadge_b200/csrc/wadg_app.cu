@@ -479,4 +479,14 @@ int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {
   return WADG_OK;
 }
 
+void *wadg_app_stream(wadg_app *a) { return a ? (void *)a->stream : nullptr; }
+
+int wadg_app_set_parity(wadg_app *a, int parity) {
+  if (!a || (parity != 0 && parity != 1)) return afail(WADG_ERR_INVALID, "invalid argument");
+  a->cur = parity;
+  return WADG_OK;
+}
+
+int wadg_app_get_fused(wadg_app *a) { return a ? a->fused : 0; }
+
 }  // extern "C"

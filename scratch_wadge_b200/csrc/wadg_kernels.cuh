@@ -175,8 +175,10 @@ struct SurfCfg {
   static constexpr size_t smem = sizeof(double) * E * El::Nfields * El::NfqNf;
 };
 
+// register cap from the launch bounds: about 1000 threads per SM (~64
+// registers each), enough warps to hide the neighbour-trace gathers
 template <int DIM, int N, int E>
-__global__ void __launch_bounds__(SurfCfg<DIM, N, E>::threads)
+__global__ void __launch_bounds__(SurfCfg<DIM, N, E>::threads, 1024 / SurfCfg<DIM, N, E>::threads)
 surf_kernel(int K, const double *__restrict__ fgeo, const uint32_t *__restrict__ mapPq,
             const double *__restrict__ VqLq, const double *__restrict__ Qf,
             const double *__restrict__ rhsQf, double *__restrict__ rhsQ, Phys P) {
