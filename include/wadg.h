@@ -246,6 +246,34 @@ int wadg_ensemble_run(wadg_ensemble *ens, double dt, int nsteps);
 int wadg_ensemble_sync(wadg_ensemble *ens);
 int wadg_ensemble_time_run(wadg_ensemble *ens, double dt, int nsteps, float *ms);
 
+/* ------------------------------------------------------------ no allocation
+ * One LSRK stage -- vol, surf and update, exactly what wadg_rk_step does --
+ * for callers that may not allocate device memory: a host program that owns
+ * all GPU memory through its own pool and passes the library only its own
+ * buffers (the way the reference's driver allocates everything up front with
+ * device_malloc), or a time loop that must not call cudaMalloc/cudaFree,
+ * which synchronise the device and can fail in the middle of a run.  No
+ * counterpart in the reference.
+ *
+ * Arguments as for the three kernels; the face-row buffer they pass between
+ * them (rhsQf) lives in a fixed device array of the library instead:
+ * WADG_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), resident on every GPU that
+ * loads the library until the process exits.  Limit: K * Nfq*Nfaces *
+ * Nfields must not exceed it (3D N=3: K <= 8738); larger K is rejected with
+ * WADG_ERR_INVALID.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race, so serialise them. */
+#define WADG_NOALLOC_SCRATCH_DOUBLES (2 * 1024 * 1024)
+int wadg_rk_stage_noalloc(wadg_ctx *ctx, int K, int curved, const double *vgeo,
+                          const double *vfgeo, const double *fgeo,
+                          const uint32_t *mapPq, const double *nrJ,
+                          const double *nsJ, const double *ntJ,
+                          const double *Drq, const double *Dsq,
+                          const double *Dtq, const double *VqLq,
+                          const double *VqPq, const double *VfPq,
+                          const double *Jq, double fa, double fb, double fdt,
+                          double *rhsQ, double *resQ, double *Q, double *Qf);
+
 /* ------------------------------------------------------------ measurement
  * FP64 FMA throughput of the current GPU (the denominator of the volume
  * kernel's FP64 roofline): a saturating FMA kernel timed with CUDA events on

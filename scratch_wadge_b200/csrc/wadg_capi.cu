@@ -230,6 +230,14 @@ namespace wadg_internal {
 void set_error(const std::string &msg) { g_err = msg; }
 }  // namespace wadg_internal
 
+// dimension and face-point count of a context (used by wadg_noalloc.cu)
+int wadg_ctx_sizes(const wadg_ctx *c, int *dim, int *NfqNf) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  *dim = c->dim;
+  *NfqNf = c->Nfq * c->Nfaces;
+  return WADG_OK;
+}
+
 extern "C" {
 
 const char *wadg_last_error(void) { return g_err.c_str(); }
