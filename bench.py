@@ -10,10 +10,15 @@ Metric: FP64 DOF*stages/s, DOF = K * Np per field (Np = 20, Nfields = 5).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A time step runs the fused stage kernel (wadg_euler_stage_3d: vol + surf +
-update in one launch per stage, 5 launches per step, replayed as a CUDA
-graph); the line also reports the three reference-facing kernels timed one by
-one.
+A time step runs either the three reference-facing kernels per stage or the
+fused stage kernel (wadg_euler_stage_3d: vol + surf + update in one launch per
+stage), whichever is faster on this GPU (both are timed, `stage_variant`),
+replayed as a CUDA graph; the line also reports the three kernels timed one by
+one (`roofline`, `hbm_kernels`).  Two more workloads are reported beside the
+headline: `ensemble` (256 independent 2D vortex solves, batched against one
+solver per instance) and `adjoint` (the checkpointed discrete adjoint of a
+200-step Taylor-Green run on 3072 tets: reverse-sweep cost over the forward
+run, and a finite-difference check of the gradient).
 
 --impl ours       the CUDA library through its C ABI; `value` is timed with
                   CUDA events around K graph-replayed time steps with the state
@@ -326,6 +331,8 @@ def run_ours(args):
             "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks}
     if not args.no_ensemble:
         line["ensemble"] = run_ensemble_measurement()
+    if not args.no_adjoint:
+        line["adjoint"] = run_adjoint_measurement()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
         sec, kind = time_cpu(geo, st0, dt, 2)
@@ -339,6 +346,81 @@ def run_ours(args):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def run_adjoint_measurement(nhex=8, nsteps=200, every=20, reps=3, fd_dirs=2):
+    """Discrete adjoint of the Taylor-Green run: gradient of J = int rho(T)^2
+    with respect to the initial state on 8^3 x 6 = 3072 affine tets, N = 3,
+    200 LSRK-45 steps, checkpoint every 20 steps.  Times (CUDA events on the
+    app's stream, best of `reps`): the plain forward run (graph-replayed), the
+    checkpointed forward run and the reverse sweep (segment recompute + stage
+    adjoints).  `fd_check`: relative difference of dJ/dQ0 . d from central
+    differences of J (step 1e-6 relative to |Q0|, J summed exactly) on
+    `fd_dirs` seeded unit-norm Gaussian directions."""
+    import torch
+
+    from scratch_wadge_b200 import capi
+    from scratch_wadge_b200 import ic as IC
+    from scratch_wadge_b200 import mesh as M
+    from scratch_wadge_b200.adjoint import Adjoint, rho2_objective
+
+    geo = M.build_geometry(M.periodic_cube(nhex), N)
+    Q0 = IC.stage0(geo, IC.initial_state(geo, "taylor_green"))[0]
+    dt = IC.time_step(geo, CFL, N, nsteps=nsteps, wave_speed=IC.max_wave_speed(Q0))[0]
+    app = capi.App(geo, False)
+    adj = Adjoint(app, nsteps, every)
+    Qd = torch.from_numpy(Q0).cuda()
+    stream = torch.cuda.ExternalStream(capi.lib().wadg_app_stream(app.h))
+
+    def timed(fn):
+        best, out = None, None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            e1.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        return best, out
+
+    QT = adj.forward(Qd, dt)
+    J, gT = rho2_objective(geo, QT)
+    adj.reverse(gT)  # warm-up
+    fwd_ckpt_ms, QT = timed(lambda: adj.forward(Qd, dt))
+    J, gT = rho2_objective(geo, QT)
+    rev_ms, g0 = timed(lambda: adj.reverse(gT))
+    adj.forward(Qd, dt)
+    plain_ms = min(app.time_run(dt, nsteps, True) for _ in range(reps))
+
+    def Jexact(Q):
+        w = np.asarray(geo.ops.wq)[None, :] * np.asarray(geo.Jq)
+        return math.fsum((w * Q[:, 0, :] ** 2).ravel())
+
+    g0n = g0.cpu().numpy()
+    eps = 1e-6 * float(np.linalg.norm(Q0))
+    rng = np.random.default_rng(20261203)
+    worst = 0.0
+    for _ in range(fd_dirs):
+        z = rng.standard_normal(Q0.shape)
+        d = z / np.linalg.norm(z)
+        Jp = Jexact(adj.forward(torch.from_numpy(Q0 + eps * d).cuda(), dt).cpu().numpy())
+        Jm = Jexact(adj.forward(torch.from_numpy(Q0 - eps * d).cuda(), dt).cpu().numpy())
+        an = float(np.sum(g0n * d))
+        worst = max(worst, abs((Jp - Jm) / (2 * eps) - an) / abs(an))
+    adj.close()
+    app.close()
+    return {"workload": f"taylor_green_3d_affine_N3_K{geo.K}_{nsteps}steps_checkpoint{every}",
+            "objective": "J = integral of rho(x,T)^2 (volume cubature)", "J": float(J),
+            "forward_ms": plain_ms, "forward_checkpointed_ms": fwd_ckpt_ms, "reverse_ms": rev_ms,
+            "adjoint_over_forward": rev_ms / plain_ms,
+            "gradient_over_forward": (fwd_ckpt_ms + rev_ms) / plain_ms,
+            "fd_check": {"directions": fd_dirs, "worst_rel_diff": worst,
+                         "step": "1e-6 relative to |Q0|"},
+            "note": "adjoint_over_forward = reverse sweep (segment recompute from checkpoints + "
+                    "stage adjoint kernels) / plain forward run; gradient_over_forward adds "
+                    "the checkpointed forward run"}
 
 
 def run_ensemble_measurement(steps=5, warmup=2):
@@ -403,6 +485,7 @@ def main():
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + steps of the device path (for ncu), no JSON line")
     args = ap.parse_args()

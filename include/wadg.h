@@ -274,6 +274,46 @@ int wadg_rk_stage_noalloc(wadg_ctx *ctx, int K, int curved, const double *vgeo,
                           const double *Jq, double fa, double fb, double fdt,
                           double *rhsQ, double *resQ, double *Q, double *Qf);
 
+/* ------------------------------------------------------------ discrete adjoint
+ * Vector-Jacobian products of the RHS and of the whole LSRK-45 run
+ * (rk_run, euler.c:3672-3738) for an app, by hand-written adjoint kernels:
+ * the log-mean flux derivative, the entropy-variable Jacobians, the
+ * Lax-Friedrichs penalty with its wave-speed max differentiated along the
+ * branch the forward evaluation took (the reference's `lamM > lamP ? lamM :
+ * lamP`), the inverse mass and the entropy projection.  The reference has no
+ * adjoint; no counterpart.
+ *
+ * All state arrays are DEVICE pointers in the [K][Nfields][Nq] layout of Q.
+ * Calls are asynchronous on the app's stream.  The adjoint object borrows
+ * the app (its operators, geometry and state buffers): destroy it before the
+ * app, and do not step the app while a forward/reverse pair is in use.
+ * Requires a conforming face pairing (mapPq(mapPq(j)) = j), checked at
+ * creation. */
+typedef struct wadg_adjoint wadg_adjoint;
+/* Tape for `nsteps` time steps with a checkpoint every `every` steps:
+ * device memory (nsteps/every + 1) Q-sized checkpoints plus 5*every stages
+ * of (Q, u~, uf~). */
+int wadg_adjoint_create(wadg_app *app, int nsteps, int every,
+                        wadg_adjoint **out);
+int wadg_adjoint_destroy(wadg_adjoint *adj);
+/* Forward run of nsteps steps of size dt from Q0 (copied into the app; the
+ * projected traces are recomputed from it), storing the checkpoints.  The
+ * app holds the final state Q(T) afterwards; QT (may be NULL) receives a
+ * copy of it. */
+int wadg_adjoint_forward(wadg_adjoint *adj, const double *Q0, double dt,
+                         double *QT);
+/* Reverse sweep: given QbarT = dJ/dQ(T), writes Qbar0 = dJ/dQ0 for the run
+ * of the last wadg_adjoint_forward.  Recomputes each segment from its
+ * checkpoint; leaves the app at Q(T). */
+int wadg_adjoint_reverse(wadg_adjoint *adj, const double *QbarT,
+                         double *Qbar0);
+/* R(Q) = Minv rhs(u~(Q), uf~(Q)), the time derivative one stage applies
+ * (the update kernel's r with the projected traces of Q). */
+int wadg_adjoint_rhs(wadg_adjoint *adj, const double *Q, double *R);
+/* Qbar = (dR/dQ)^T w at Q. */
+int wadg_adjoint_rhs_vjp(wadg_adjoint *adj, const double *Q, const double *w,
+                         double *Qbar);
+
 /* ------------------------------------------------------------ measurement
  * FP64 FMA throughput of the current GPU (the denominator of the volume
  * kernel's FP64 roofline): a saturating FMA kernel timed with CUDA events on

@@ -60,6 +60,35 @@ class _Base:
         for s in range(5):
             self.stage(geo, RK4A[s], RK4B[s], dt, st)
 
+    def project(self, geo, Q):
+        """The projected traces (u~, uf~) of Q: the update kernel with a zero
+        RHS and zero coefficients leaves Q and writes U(VqPq v~), U(VfPq v~)."""
+        K, Nf, NF = Q.shape[0], Q.shape[1], self.ops.NfqNf
+        rhsQ, resQ = np.zeros_like(Q), np.zeros_like(Q)
+        Qc, Qf = np.ascontiguousarray(Q, dtype=np.float64).copy(), np.zeros((K, Nf, NF))
+        self.update(geo, 0.0, 0.0, 0.0, rhsQ, resQ, Qc, Qf)
+        return rhsQ, Qf
+
+    def rhs(self, geo, Q):
+        """R(Q) = Minv rhs(u~(Q), uf~(Q)): the update's r for the state Q
+        (res = 0 * res + 1 * r)."""
+        rhsQ, Qf = self.project(geo, Q)
+        rhsQf = np.zeros_like(Qf)
+        self.vol(geo, Qf, rhsQ, rhsQf)
+        self.surf(geo, Qf, rhsQf, rhsQ)
+        resQ, Qc = np.zeros_like(Q), np.ascontiguousarray(Q, dtype=np.float64).copy()
+        self.update(geo, 0.0, 0.0, 1.0, rhsQ, resQ, Qc, Qf)
+        return resQ
+
+    def run(self, geo, Q0, dt, nsteps):
+        """nsteps LSRK-45 steps from Q0, the traces projected from Q0."""
+        rhsQ, Qf = self.project(geo, Q0)
+        st = dict(Q=np.ascontiguousarray(Q0, dtype=np.float64).copy(), rhsQ=rhsQ, Qf=Qf,
+                  resQ=np.zeros_like(rhsQ), rhsQf=np.zeros_like(Qf))
+        for _ in range(nsteps):
+            self.step(geo, dt, st)
+        return st["Q"]
+
 
 class Port(_Base):
     """oracle/wadg_ref.c (restatement)."""

@@ -92,6 +92,12 @@ def lib():
         L.wadg_app_destroy.argtypes = [v]
         L.wadg_app_sync.argtypes = [v]
         L.wadg_ctx_set_stream.argtypes = [v, v]
+        L.wadg_adjoint_create.argtypes = [v, i, i, ctypes.POINTER(ctypes.c_void_p)]
+        L.wadg_adjoint_destroy.argtypes = [v]
+        L.wadg_adjoint_forward.argtypes = [v, v, d, v]
+        L.wadg_adjoint_reverse.argtypes = [v, v, v]
+        L.wadg_adjoint_rhs.argtypes = [v, v, v]
+        L.wadg_adjoint_rhs_vjp.argtypes = [v, v, v, v]
         _lib = L
     return _lib
 
@@ -186,6 +192,7 @@ class App:
                         [k["mapPq"].ctypes.data_as(_U32)] +
                         [_dp(k[n]) for n in ("nrJ", "nsJ", "ntJ", "Drq", "Dsq", "Dtq", "VqLq", "VqPq", "VfPq")]))
         h = ctypes.c_void_p()
+        self._destroy = lib().wadg_app_destroy  # kept for close() at interpreter exit
         check(lib().wadg_app_create(ctypes.byref(self.p), self.K, int(self.curved), ctypes.byref(hd),
                                     ctypes.byref(h)), "wadg_app_create")
         self.h = h
@@ -193,8 +200,11 @@ class App:
         self.vshape, self.fshape = (self.K, Nf, Nq), (self.K, Nf, NfqNf)
 
     def close(self):
+        # adjoints borrow the app's buffers: release them first
+        for adj in list(getattr(self, "_dependents", ())):
+            adj.close()
         if getattr(self, "h", None):
-            lib().wadg_app_destroy(self.h)
+            self._destroy(self.h)
             self.h = None
 
     __del__ = close

@@ -1,0 +1,724 @@
+// Discrete adjoint of one LSRK stage of the entropy-stable RHS: device kernels.
+//
+// The stage (rk_step, euler.c:3610-3666, with the three kernels of
+// Euler3Daffine.okl / Euler3D.okl / Euler2D.okl) maps (Q, res) to
+//   res' = a res + dt R(Q),   Q' = Q + b res',
+//   R(Q) = Minv rhs(u~(Q), uf~(Q)),
+// where u~ = U(VqPq V(Q)) and uf~ = U(VfPq V(Q)) are the entropy-projected
+// traces the previous update wrote (the WADG projection on curved elements),
+// rhs is the volume + surface flux differencing and Minv the affine or
+// weight-adjusted inverse mass.  Its adjoint, given (Qbar', resbar'):
+//   r = resbar' + b Qbar',  resbar = a r,  Qbar = Qbar' + (dR/dQ)^T (dt r).
+// Three kernels evaluate it:
+//   adj_seed_kernel   w = dt r, rhsbar = Minv^T w, sfbar = VqLq^T rhsbar
+//                     (the adjoint of the lift rhsQ += VqLq sf)
+//   adj_pairs_kernel  the VJP of every two-point flux evaluation (volume-volume,
+//                     volume-face and surface, with the Lax-Friedrichs
+//                     penalty), then the adjoints of the primitive recovery
+//                     and of U(V~) at each volume and face node: vbar, vfbar
+//   adj_proj_kernel   the adjoint of the entropy projection and of V(Q), and
+//                     the LSRK adjoint update of Qbar and resbar.
+// Neighbour contributions of the surface term are gathered, not scattered:
+// face node j adds the P-side derivative of the evaluation made at its
+// neighbour m = mapPq(j), which needs sfbar at m (hence the separate seed
+// kernel) and mapPq(m) = j (a conforming face pairing; checked on the host).
+#pragma once
+
+#include "wadg_adjoint_math.cuh"
+#include "wadg_device.cuh"
+#include "wadg_vol.cuh"
+
+namespace wadg {
+
+// node state of the pair VJP: NodeState plus 1/rho and 1/beta
+template <int DIM> struct AdjNode {
+  double rho, vel[DIM], beta, lrho, lbeta, irho, ibeta;
+};
+
+// F(u) = sum_{k<=8} u^k/(2k+1) and dF/du
+__device__ __forceinline__ void polyF_d(double u, double &F, double &dF) {
+  const double c[9] = {1.0, 1.0 / 3.0, 1.0 / 5.0, 1.0 / 7.0, 1.0 / 9.0,
+                       1.0 / 11.0, 1.0 / 13.0, 1.0 / 15.0, 1.0 / 17.0};
+  F = c[8];
+  dF = 0.0;
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    dF = fma(dF, u, F);
+    F = fma(F, u, c[k]);
+  }
+}
+// G(u) = 1/F(u) to degree 8 (the coefficients of polyG) and dG/du
+__device__ __forceinline__ void polyG_d(double u, double &G, double &dG) {
+  const double c[9] = {1.0, -1.0 / 3.0, -4.0 / 45.0, -44.0 / 945.0, -428.0 / 14175.0,
+                       -10196.0 / 467775.0, -10719068.0 / 638512875.0,
+                       -25865068.0 / 1915538625.0, -5472607916.0 / 488462349375.0};
+  G = c[8];
+  dG = 0.0;
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    dG = fma(dG, u, G);
+    G = fma(G, u, c[k]);
+  }
+}
+
+// Vector-Jacobian product of the contracted two-point flux F_S(a, b).n
+// (ecflux_n; Euler3Daffine.okl:107-148, Euler2D.okl:139-161) with the
+// adjoint c of its Nfields components.  Adds the adjoints of a's and b's
+// primitive states (rho, velocity, beta) to ba and bb.
+//
+// Log-mean derivatives (L(a,b) = (a-b)/(log a - log b), s = a+b, f = (a-b)/s,
+// u = f^2):
+//   log form:    dL/da = (1 - L/a)/(log a - log b), dL/db = (L/b - 1)/(log a - log b)
+//   series form: L = s/2 G(u): dL/da = G/2 + G'(u) f (1-f), dL/db = G/2 - G' f (1+f)
+// and for 1/L (the inverse-temperature mean, 1/L = 2F(u)/s):
+//   log form:    d(1/L)/da = (1/a - 1/L)/(a-b), d(1/L)/db = (1/L - 1/b)/(a-b)
+//   series form: d(1/L)/da = 2/s^2 (-F + 2F' f(1-f)), d(1/L)/db = 2/s^2 (-F - 2F' f(1+f))
+// with the same branch switch (u < 1e-2) as the forward flux.
+template <int DIM>
+__device__ __forceinline__ void ecflux_vjp(const AdjNode<DIM> &a, const AdjNode<DIM> &b,
+                                           const double *n, const double *c, const Phys &P,
+                                           double *ba, double *bb) {
+  const double sr = a.rho + b.rho, dr = a.rho - b.rho;
+  const double sb = a.beta + b.beta, db = a.beta - b.beta;
+  const double isr = rcp(sr), isb = rcp(sb);
+  const double fr = dr * isr, fb = db * isb;
+  const double ur = fr * fr, ub = fb * fb;
+  double rl, rla, rlb, ibl, ibla, iblb;
+  if (ur < 1e-2) {
+    double G, dG;
+    polyG_d(ur, G, dG);
+    rl = 0.5 * sr * G;
+    const double t = dG * fr;
+    rla = fma(-t, fr, fma(0.5, G, t));
+    rlb = fma(-t, fr, fma(0.5, G, -t));
+  } else {
+    const double ild = rcp(a.lrho - b.lrho);
+    rl = dr * ild;
+    rla = fma(-rl, a.irho, 1.0) * ild;
+    rlb = fma(rl, b.irho, -1.0) * ild;
+  }
+  if (ub < 1e-2) {
+    double F, dF;
+    polyF_d(ub, F, dF);
+    ibl = 2.0 * isb * F;
+    const double t2 = 2.0 * isb * isb, t = 2.0 * dF * fb;
+    ibla = t2 * (fma(-t, fb, t) - F);
+    iblb = t2 * (fma(-t, fb, -t) - F);
+  } else {
+    const double idb = rcp(db);
+    ibl = (a.lbeta - b.lbeta) * idb;
+    ibla = (a.ibeta - ibl) * idb;
+    iblb = (ibl - b.ibeta) * idb;
+  }
+  const double pa = 0.5 * sr * isb;
+  double ubar[DIM], un = 0.0, vv = 0.0, cu = 0.0, cn = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    ubar[d] = 0.5 * (a.vel[d] + b.vel[d]);
+    un = fma(ubar[d], n[d], un);
+    vv = fma(a.vel[d], b.vel[d], vv);
+    cu = fma(c[1 + d], ubar[d], cu);
+    cn = fma(c[1 + d], n[d], cn);
+  }
+  const double h = fma(ibl, P.cbeta, 0.5 * vv);
+  const double f4 = fma(rl, h, pa);
+  const double F0 = rl * un;
+  const double cE = c[DIM + 1];
+  // reverse sweep
+  const double F0b = c[0] + cu;
+  const double f4b = cE * un;
+  const double unb = fma(F0b, rl, cE * f4);
+  const double rlbar = fma(F0b, un, f4b * h);
+  const double iblbar = f4b * rl * P.cbeta;
+  const double vvb = 0.5 * f4b * rl;
+  const double pab = cn + f4b;
+  const double prho = 0.5 * pab * isb, pbeta = -pab * pa * isb;
+  ba[0] = fma(rlbar, rla, ba[0] + prho);
+  bb[0] = fma(rlbar, rlb, bb[0] + prho);
+  ba[DIM + 1] = fma(iblbar, ibla, ba[DIM + 1] + pbeta);
+  bb[DIM + 1] = fma(iblbar, iblb, bb[DIM + 1] + pbeta);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double hb = 0.5 * fma(c[1 + d], F0, unb * n[d]);
+    ba[1 + d] = fma(vvb, b.vel[d], ba[1 + d] + hb);
+    bb[1 + d] = fma(vvb, a.vel[d], bb[1 + d] + hb);
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ AdjNode<DIM> adj_node(const double *q, int stride, const Phys &P) {
+  const NodeState<DIM> s = node_state<DIM>(q, stride, P);
+  AdjNode<DIM> a;
+  a.rho = s.rho;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) a.vel[d] = s.vel[d];
+  a.beta = s.beta;
+  a.lrho = s.lrho;
+  a.lbeta = s.lbeta;
+  a.irho = 1.0 / s.rho;
+  a.ibeta = 1.0 / s.beta;
+  return a;
+}
+
+__device__ __forceinline__ adj::Gas gas_of(const Phys &P) {
+  return adj::Gas{P.gamma, P.gm1, P.cbeta, P.lgm1, P.igm1};
+}
+
+// ------------------------------------------------------------------ seed
+// w = dt (resbar + b Qbar); rhsbar = Minv^T w; sfbar = VqLq^T rhsbar.
+//   affine Minv = -2 diag(1/J) VqPq    (Euler3Daffine.okl:555-620)
+//   WADG   Minv = VqPq diag(1/J) (-2 VqPq)   (Euler3D.okl:2527-2620)
+template <int DIM, int N, int E> struct AdjSeedCfg {
+  using El = Elem<DIM, N>;
+  static constexpr int threads = E * El::Nq;
+  static constexpr size_t smem = sizeof(double) * 2 * E * El::Nfields * El::Nq;
+};
+
+template <int DIM, int N, bool CURVED, int E>
+__global__ void __launch_bounds__(AdjSeedCfg<DIM, N, E>::threads)
+adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
+                const double *__restrict__ VqLq, double b, double dt,
+                const double *__restrict__ Qbar, const double *__restrict__ resbar,
+                double *__restrict__ rhsbar, double *__restrict__ sfbar) {
+  using El = Elem<DIM, N>;
+  constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
+  extern __shared__ double smem[];
+  double (*sA)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
+  double (*sB)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
+  const int k0 = blockIdx.x * E;
+  const int kend = min(K - k0, E);
+  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
+  const bool valid = e < kend;
+  const size_t id = (size_t)k * Nq * Nf + i;
+  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
+
+  // transposed matvec: out[f] = sum_j Op(j, row) X[f][j]  (Op column-major, ld rows)
+  auto matvecT = [&](const double *Op, int ld, int row, double (*X)[Nq], double *out) {
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f] = 0.0;
+    for (int j = 0; j < Nq; ++j) {
+      const double w = __ldg(Op + j + row * ld);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) out[f] = fma(w, X[f][j], out[f]);
+    }
+  };
+
+  if (valid) {
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) {
+      const double w = dt * fma(b, Qbar[id + f * Nq], resbar[id + f * Nq]);
+      sA[e][f][i] = CURVED ? w : -2.0 * w / Jqi;
+    }
+  }
+  __syncthreads();
+  double r[Nf];
+  if (CURVED) {
+    if (valid) {
+      matvecT(VqPq, Nq, i, sA[e], r);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) sB[e][f][i] = -2.0 * r[f] / Jqi;
+    }
+    __syncthreads();
+    if (valid) matvecT(VqPq, Nq, i, sB[e], r);
+    __syncthreads();
+  } else if (valid) {
+    matvecT(VqPq, Nq, i, sA[e], r);
+  }
+  if (valid) {
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) {
+      rhsbar[id + f * Nq] = r[f];
+      sB[e][f][i] = r[f];
+    }
+  }
+  __syncthreads();
+  // sfbar(f) = sum_i VqLq(i, f) rhsbar(i)
+  for (int t = threadIdx.x; t < kend * NF; t += blockDim.x) {
+    const int ee = t / NF, fn = t % NF;
+    double s[Nf];
+    matvecT(VqLq, Nq, fn, sB[ee], s);
+    double *out = sfbar + (size_t)(k0 + ee) * NF * Nf + fn;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) out[f * NF] = s[f];
+  }
+}
+
+// ------------------------------------------------------------------ pairs
+// Layout as the pair-scheduled volume kernel (wadg_vol.cuh): a group of L
+// lanes owns an element, lane l owns the volume rows i = l + L r, whose state,
+// seed rhsbar(i) and primitive adjoint stay in registers.  The column partner
+// of a step is staggered, j = j0 + (l + s) mod n, so the L lanes of a group
+// touch L distinct columns and add their column adjoints to shared memory
+// without conflicts (__syncwarp between steps).  With H = 2 the two warps of
+// an element take disjoint halves of the columns, so they never write the
+// same column; the row adjoints of the two warps are combined at the end.
+// Every ordered volume pair (i, j) is one VJP (seed rhsbar(i), direction
+// D_ij); every volume-face pair (i, f) is one VJP with the combined seed
+// 1/2 VqLq(i,f) rhsbar(i) - 1/2 VfPq(f,i) sfbar(f), the two uses of that
+// flux in the forward volume kernel.
+template <int DIM, int N, bool CURVED, int W>
+struct AdjPairsCfg {
+  using El = Elem<DIM, N>;
+  using T = VolTile<DIM, N>;
+  static constexpr int Nq = El::Nq, NF = El::NfqNf, NN = El::NN, Nf = El::Nfields;
+  static constexpr int L = T::L, R = T::R, G = T::G;
+  static constexpr int nv0 = (Nq + 1) / 2, nv1 = Nq - nv0, nf0 = (NF + 1) / 2, nf1 = NF - nf0;
+  static constexpr int H = (nv1 >= L && nf1 >= L) ? 2 : 1;
+  static constexpr int NSA = DIM + 6;               // AdjNode fields
+  static constexpr int NGS = CURVED ? El::Nvgeo : 0; // geometric factors per node
+  static constexpr int NB = DIM + 2;                // primitive adjoint components
+  static constexpr int threads = 32 * W;
+  static constexpr int E = (W / H) * T::G;
+  static constexpr int pad4of8(int x) { return ((x + 3) / 8) * 8 + 4; }
+  static constexpr int SST = (NSA + NGS) * NN;  // node states (+ geometric factors)
+  static constexpr int SSF = Nf * NF;           // sfbar of the face nodes
+  static constexpr int SBR = NB * NN;           // column adjoints
+  static constexpr int SN = El::Nfaces * DIM + El::Nvgeo;
+  static constexpr int per_elem = pad4of8(SST + SSF + SBR + SN);
+  static constexpr int nTD = DIM * R * Nq * L;
+  static constexpr int nTW = R * NF * L;
+  static constexpr size_t fixed = sizeof(double) * (size_t)(nTD + 2 * nTW + El::Nfaces * DIM);
+  static constexpr size_t smem = fixed + sizeof(double) * (size_t)E * per_elem;
+  static_assert(W % H == 0, "warps per CTA must be a multiple of the warps per element");
+};
+
+template <int DIM, int N, bool CURVED, int W>
+__global__ void __launch_bounds__(32 * W, 1)
+adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
+                 const double *__restrict__ fgeo, const uint32_t *__restrict__ mapPq,
+                 const double *__restrict__ nrJ, const double *__restrict__ nsJ,
+                 const double *__restrict__ ntJ, const double *__restrict__ Drq,
+                 const double *__restrict__ Dsq, const double *__restrict__ Dtq,
+                 const double *__restrict__ VqLq, const double *__restrict__ VfPq,
+                 const double *__restrict__ uq, const double *__restrict__ uf,
+                 const double *__restrict__ rhsbar, const double *__restrict__ sfbar,
+                 double *__restrict__ vbar, double *__restrict__ vfbar, Phys P) {
+  using C = AdjPairsCfg<DIM, N, CURVED, W>;
+  using El = Elem<DIM, N>;
+  constexpr int Nq = C::Nq, NF = C::NF, NN = C::NN, Nf = C::Nf, L = C::L, R = C::R, G = C::G;
+  constexpr int H = C::H, E = C::E, NSA = C::NSA, NB = C::NB, NG = El::Nvgeo, Nfq = El::Nfq;
+  constexpr int NFG = El::Nfgeo;
+  extern __shared__ double smem[];
+  double *tD = smem;                 // [h][a][r][s][l]
+  double *tW1 = tD + C::nTD;         // [h][r][s][l]  1/2 VqLq(i, f)
+  double *tW2 = tW1 + C::nTW;        // [h][r][s][l] -1/2 VfPq(f, i)
+  double *sNr = tW2 + C::nTW;        // [Nfaces][DIM]
+  double *sEl = sNr + El::Nfaces * DIM;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int h = warp % H, g = lane / L, l = lane % L;
+  const int e = (warp / H) * G + g;
+  auto nv = [](int hh) { return H == 1 ? Nq : (hh ? C::nv1 : C::nv0); };
+  auto nf = [](int hh) { return H == 1 ? NF : (hh ? C::nf1 : C::nf0); };
+  auto cv = [](int hh) { return hh ? C::nv0 : 0; };
+  auto cf = [](int hh) { return hh ? C::nf0 : 0; };
+
+  // tables
+  for (int t = tid; t < C::nTD; t += blockDim.x) {
+    int hh = 0, u = t;
+    if (H == 2 && u >= DIM * R * L * C::nv0) {
+      hh = 1;
+      u -= DIM * R * L * C::nv0;
+    }
+    const int n_ = nv(hh);
+    const int ll = u % L, s = (u / L) % n_, r = (u / (L * n_)) % R, a = u / (L * n_ * R);
+    const int i = ll + L * r;
+    int jj = ll + s;
+    if (jj >= n_) jj -= n_;
+    const int j = cv(hh) + jj;
+    const double *D = a == 0 ? Drq : (a == 1 ? Dsq : Dtq);
+    tD[t] = i < Nq ? D[i + j * Nq] : 0.0;
+  }
+  for (int t = tid; t < C::nTW; t += blockDim.x) {
+    int hh = 0, u = t;
+    if (H == 2 && u >= R * L * C::nf0) {
+      hh = 1;
+      u -= R * L * C::nf0;
+    }
+    const int n_ = nf(hh);
+    const int ll = u % L, s = (u / L) % n_, r = u / (L * n_);
+    const int i = ll + L * r;
+    int ff = ll + s;
+    if (ff >= n_) ff -= n_;
+    const int f = cf(hh) + ff;
+    tW1[t] = i < Nq ? 0.5 * VqLq[i + f * Nq] : 0.0;
+    tW2[t] = i < Nq ? -0.5 * VfPq[f + i * NF] : 0.0;
+  }
+  for (int t = tid; t < El::Nfaces; t += blockDim.x) {
+    sNr[t * DIM + 0] = nrJ[t * Nfq];
+    sNr[t * DIM + 1] = nsJ[t * Nfq];
+    if (DIM == 3) sNr[t * DIM + 2] = ntJ[t * Nfq];
+  }
+  const double *tDh = tD + DIM * R * L * cv(h);
+  const double *tW1h = tW1 + R * L * cf(h), *tW2h = tW2 + R * L * cf(h);
+  const adj::Gas gas = gas_of(P);
+
+  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
+    __syncthreads();  // tables ready / previous batch done with shared memory
+    // ---- prologue: node states, face seeds, zeroed column adjoints, normals
+    for (int t = tid; t < E * NN; t += blockDim.x) {
+      const int ee = t / NN, n = t % NN;
+      const int k = min(k0 + ee, K - 1);
+      const AdjNode<DIM> s = (n < Nq) ? adj_node<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
+                                      : adj_node<DIM>(uf + (size_t)k * NF * Nf + (n - Nq), NF, P);
+      double *st = sEl + ee * C::per_elem;
+      st[0 * NN + n] = s.rho;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = s.vel[d];
+      st[(DIM + 1) * NN + n] = s.beta;
+      st[(DIM + 2) * NN + n] = s.lrho;
+      st[(DIM + 3) * NN + n] = s.lbeta;
+      st[(DIM + 4) * NN + n] = s.irho;
+      st[(DIM + 5) * NN + n] = s.ibeta;
+      if (CURVED) {
+#pragma unroll
+        for (int c = 0; c < NG; ++c)
+          st[(NSA + c) * NN + n] = (n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
+                                            : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
+      }
+    }
+    for (int t = tid; t < E * C::SSF; t += blockDim.x) {
+      const int ee = t / C::SSF, u = t % C::SSF;
+      const int k = min(k0 + ee, K - 1);
+      sEl[ee * C::per_elem + C::SST + u] = sfbar[(size_t)k * NF * Nf + u];
+    }
+    for (int t = tid; t < E * C::SBR; t += blockDim.x) {
+      const int ee = t / C::SBR, u = t % C::SBR;
+      sEl[ee * C::per_elem + C::SST + C::SSF + u] = 0.0;
+    }
+    if (!CURVED) {
+      for (int t = tid; t < E; t += blockDim.x) {
+        const int k = min(k0 + t, K - 1);
+        double Gk[NG];
+#pragma unroll
+        for (int c = 0; c < NG; ++c) Gk[c] = vgeo[(size_t)k * Nq * NG + c * Nq];  // node 0 (:205)
+        double *nm = sEl + t * C::per_elem + C::SST + C::SSF + C::SBR;
+#pragma unroll
+        for (int c = 0; c < NG; ++c) nm[El::Nfaces * DIM + c] = Gk[c];
+        for (int fc = 0; fc < El::Nfaces; ++fc)
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            double v = 0.0;
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) v = fma(Gk[a * DIM + d], sNr[fc * DIM + a], v);
+            nm[fc * DIM + d] = v;
+          }
+      }
+    }
+    __syncthreads();
+
+    // ---- pairs
+    const double *st = sEl + e * C::per_elem;
+    const double *sfb = st + C::SST;
+    double *bar = sEl + e * C::per_elem + C::SST + C::SSF;
+    const double *nm = st + C::SST + C::SSF + C::SBR;
+    auto load = [&](int n) {
+      AdjNode<DIM> s;
+      s.rho = st[n];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) s.vel[d] = st[(1 + d) * NN + n];
+      s.beta = st[(DIM + 1) * NN + n];
+      s.lrho = st[(DIM + 2) * NN + n];
+      s.lbeta = st[(DIM + 3) * NN + n];
+      s.irho = st[(DIM + 4) * NN + n];
+      s.ibeta = st[(DIM + 5) * NN + n];
+      return s;
+    };
+    const int kq = min(k0 + e, K - 1);
+    AdjNode<DIM> A[R];
+    int ir[R];
+    double cr[R][Nf], rb[R][NB];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = l + L * r;
+      ir[r] = min(i, Nq - 1);  // padding row: clamped state, zero seed
+      A[r] = load(ir[r]);
+#pragma unroll
+      for (int q = 0; q < Nf; ++q)
+        cr[r][q] = i < Nq ? rhsbar[(size_t)kq * Nq * Nf + q * Nq + i] : 0.0;
+#pragma unroll
+      for (int q = 0; q < NB; ++q) rb[r][q] = 0.0;
+    }
+    double Ge[NG];
+    if (!CURVED) {
+#pragma unroll
+      for (int c = 0; c < NG; ++c) Ge[c] = nm[El::Nfaces * DIM + c];
+    }
+
+    // volume-volume pairs over this warp's column half
+    {
+      const int n_ = nv(h), j0 = cv(h);
+      for (int s = 0; s < n_; ++s) {
+        int jj = l + s;
+        if (jj >= n_) jj -= n_;
+        const int j = j0 + jj;
+        const AdjNode<DIM> B = load(j);
+        double cb[NB];
+#pragma unroll
+        for (int q = 0; q < NB; ++q) cb[q] = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          double rr[DIM], nvd[DIM];
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) rr[a] = tDh[((a * R + r) * n_ + s) * L + l];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            double v = 0.0;
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) {
+              const double gad = CURVED ? 0.5 * (st[(NSA + a * DIM + d) * NN + ir[r]] +
+                                                 st[(NSA + a * DIM + d) * NN + j])
+                                        : Ge[a * DIM + d];
+              v = fma(gad, rr[a], v);
+            }
+            nvd[d] = v;
+          }
+          ecflux_vjp<DIM>(A[r], B, nvd, cr[r], P, rb[r], cb);
+        }
+#pragma unroll
+        for (int q = 0; q < NB; ++q) bar[q * NN + j] += cb[q];
+        __syncwarp();
+      }
+    }
+    // volume-face pairs over this warp's face half
+    {
+      const int n_ = nf(h), f0 = cf(h);
+      for (int s = 0; s < n_; ++s) {
+        int ff = l + s;
+        if (ff >= n_) ff -= n_;
+        const int f = f0 + ff;
+        const AdjNode<DIM> B = load(Nq + f);
+        const int fc = f / Nfq;
+        double cfs[Nf], nvd[DIM];
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) cfs[q] = sfb[q * NF + f];
+        if (!CURVED) {
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) nvd[d] = nm[fc * DIM + d];
+        }
+        double cb[NB];
+#pragma unroll
+        for (int q = 0; q < NB; ++q) cb[q] = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (CURVED) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+              double v = 0.0;
+#pragma unroll
+              for (int a = 0; a < DIM; ++a)
+                v = fma(0.5 * (st[(NSA + a * DIM + d) * NN + ir[r]] +
+                               st[(NSA + a * DIM + d) * NN + Nq + f]),
+                        sNr[fc * DIM + a], v);
+              nvd[d] = v;
+            }
+          }
+          const double w1 = tW1h[(r * n_ + s) * L + l];
+          const double w2 = tW2h[(r * n_ + s) * L + l];
+          double c[Nf];
+#pragma unroll
+          for (int q = 0; q < Nf; ++q) c[q] = fma(w1, cr[r][q], w2 * cfs[q]);
+          ecflux_vjp<DIM>(A[r], B, nvd, c, P, rb[r], cb);
+        }
+#pragma unroll
+        for (int q = 0; q < NB; ++q) bar[q * NN + Nq + f] += cb[q];
+        __syncwarp();
+      }
+    }
+    // row adjoints into the column adjoints, one warp of the element at a time
+#pragma unroll
+    for (int hh = 0; hh < H; ++hh) {
+      __syncthreads();
+      if (h == hh) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = l + L * r;
+          if (i < Nq) {
+#pragma unroll
+            for (int q = 0; q < NB; ++q) bar[q * NN + i] += rb[r][q];
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- per node: surface term (face nodes), primitive recovery and U(V~) adjoints
+    for (int t = tid; t < E * NN; t += blockDim.x) {
+      const int ee = t / NN, n = t % NN, k = k0 + ee;
+      if (k >= K) continue;
+      const double *bt = sEl + ee * C::per_elem + C::SST + C::SSF;
+      adj::PrimBar<DIM> pb;
+      pb.rho = bt[n];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) pb.u[d] = bt[(1 + d) * NN + n];
+      pb.beta = bt[(DIM + 1) * NN + n];
+      double U[Nf], Ub[Nf], Vv[Nf], Vb[Nf];
+      if (n < Nq) {
+        const double *q = uq + (size_t)k * Nq * Nf + n;
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) U[f] = q[f * Nq];
+        adj::prim_vjp<DIM>(U, pb, gas, Ub);
+      } else {
+        // surface flux + Lax-Friedrichs penalty (Euler3Daffine.okl:421-552,
+        // Euler3D.okl:3242-3473, Euler2D.okl:1357-1495):
+        //   sf_j = 1/2 F_S(u_j, u_P).nJ_j - tau/4 max(lam_j, lam_P) sJ_j (u_P - u_j)
+        // own evaluation (j as the minus side) and the neighbour's (j as its plus side)
+        const int j = n - Nq;
+        const size_t idM = (size_t)k * NF * Nf + j;
+        const size_t idP = mapPq[(size_t)k * NF + j];
+        const size_t eP = idP / (size_t)(NF * Nf), jP = idP - eP * (size_t)(NF * Nf);
+        double UP[Nf], cM[Nf], cP[Nf], nM[DIM], nP[DIM];
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) {
+          U[f] = uf[idM + f * NF];
+          UP[f] = uf[idP + f * NF];
+          cM[f] = bt[-C::SSF + f * NF + j];  // this element's sfbar, staged in shared memory
+          cP[f] = sfbar[idP + f * NF];
+        }
+        const double *fgM = fgeo + (size_t)k * NF * NFG + j;
+        const double *fgP = fgeo + eP * NF * NFG + jP;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          nM[d] = 0.5 * fgM[d * NF];
+          nP[d] = 0.5 * fgP[d * NF];
+        }
+        const double sJM = fgM[DIM * NF], sJP = fgP[DIM * NF];
+        const adj::Prim<DIM> pM = adj::prim<DIM>(U, gas), pP = adj::prim<DIM>(UP, gas);
+        adj::PrimBar<DIM> dummy;
+        adj::zero(dummy);
+        adj::flux_vjp<DIM>(pM, pP, nM, gas, cM, pb, dummy);  // own: j is a
+        adj::flux_vjp<DIM>(pP, pM, nP, gas, cP, dummy, pb);  // neighbour's: j is b
+        adj::prim_vjp<DIM>(U, pb, gas, Ub);
+        double dlM[Nf], dlP[Nf];
+        const double lamM = adj::lambda_d<DIM>(U, gas, dlM);
+        const double lamP = adj::lambda_d<DIM>(UP, gas, dlP);
+        const double tq = (DIM == 3 ? P.tau : 1.0) * 0.25;
+        const double lmax = fmax(lamM, lamP);
+        double LbM = 0.0, LbP = 0.0;
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) {
+          const double du = UP[f] - U[f];
+          Ub[f] += tq * lmax * (sJM * cM[f] - sJP * cP[f]);
+          LbM -= cM[f] * du;   // adjoint of the own penalty scale
+          LbP += cP[f] * du;   // ... and of the neighbour's (its jump is u_j - u_P)
+        }
+        // the max takes the branch the forward took: own lam_j > lam_P picks j;
+        // at the neighbour, lam_P > lam_j picks the neighbour, otherwise j
+        const double gsel = (lamM > lamP ? LbM * sJM : 0.0) + (lamP > lamM ? 0.0 : LbP * sJP);
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) Ub[f] = fma(tq * gsel, dlM[f], Ub[f]);
+      }
+      adj::V_of_U<DIM>(U, gas, Vv);
+      adj::UV_vjp<DIM>(Vv, Ub, gas, Vb);
+      if (n < Nq) {
+        double *o = vbar + (size_t)k * Nq * Nf + n;
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) o[f * Nq] = Vb[f];
+      } else {
+        double *o = vfbar + (size_t)k * NF * Nf + (n - Nq);
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) o[f * NF] = Vb[f];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ projection
+// Adjoint of the entropy projection and of V(Q), then the LSRK adjoint update.
+//   affine: u~ = U(VqPq v), uf~ = U(VfPq v), v = V(Q)
+//   WADG:   v~ = VqPq((VqPq (v J)) / J), u~ = U(VqPq v~), uf~ = U(VfPq v~)
+// X = VqPq^T vbar + VfPq^T vfbar;  affine: v-bar = X;
+// WADG: v-bar = J VqPq^T((VqPq^T X) / J);  Qbar += dV/dQ^T v-bar.
+template <int DIM, int N, int E> struct AdjProjCfg {
+  using El = Elem<DIM, N>;
+  static constexpr int threads = E * El::Nq;
+  static constexpr size_t smem = sizeof(double) * E * El::Nfields * (2 * El::Nq + El::NfqNf);
+};
+
+template <int DIM, int N, bool CURVED, int E>
+__global__ void __launch_bounds__(AdjProjCfg<DIM, N, E>::threads)
+adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
+                const double *__restrict__ VfPq, const double *__restrict__ Qs,
+                const double *__restrict__ vbar, const double *__restrict__ vfbar, double a,
+                double b, double *__restrict__ Qbar, double *__restrict__ resbar, Phys P) {
+  using El = Elem<DIM, N>;
+  constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
+  extern __shared__ double smem[];
+  double (*sV)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
+  double (*sX)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
+  double (*sVf)[Nf][NF] = reinterpret_cast<double (*)[Nf][NF]>(smem + 2 * E * Nf * Nq);
+  const int k0 = blockIdx.x * E;
+  const int kend = min(K - k0, E);
+  {
+    const double *src = vbar + (size_t)k0 * Nf * Nq;
+    for (int t = threadIdx.x; t < kend * Nf * Nq; t += blockDim.x) (&sV[0][0][0])[t] = src[t];
+    const double *srf = vfbar + (size_t)k0 * Nf * NF;
+    for (int t = threadIdx.x; t < kend * Nf * NF; t += blockDim.x) (&sVf[0][0][0])[t] = srf[t];
+  }
+  __syncthreads();
+  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
+  const bool valid = e < kend;
+  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
+
+  double x[Nf];
+#pragma unroll
+  for (int f = 0; f < Nf; ++f) x[f] = 0.0;
+  if (valid) {
+    for (int j = 0; j < Nq; ++j) {
+      const double w = __ldg(VqPq + j + i * Nq);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) x[f] = fma(w, sV[e][f][j], x[f]);
+    }
+    for (int j = 0; j < NF; ++j) {
+      const double w = __ldg(VfPq + j + i * NF);
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) x[f] = fma(w, sVf[e][f][j], x[f]);
+    }
+  }
+  if (CURVED) {
+    // y = VqPq^T x / J ; z = VqPq^T y ; vbar = J z
+    if (valid)
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) sX[e][f][i] = x[f];
+    __syncthreads();
+    double y[Nf];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) y[f] = 0.0;
+    if (valid) {
+      for (int j = 0; j < Nq; ++j) {
+        const double w = __ldg(VqPq + j + i * Nq);
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) y[f] = fma(w, sX[e][f][j], y[f]);
+      }
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) sV[e][f][i] = y[f] / Jqi;  // sV is free: read before the first barrier
+    }
+    __syncthreads();
+    if (valid) {
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) x[f] = 0.0;
+      for (int j = 0; j < Nq; ++j) {
+        const double w = __ldg(VqPq + j + i * Nq);
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) x[f] = fma(w, sV[e][f][j], x[f]);
+      }
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) x[f] *= Jqi;
+    }
+  }
+  if (!valid) return;
+  const size_t id = (size_t)k * Nq * Nf + i;
+  double U[Nf], Ub[Nf];
+#pragma unroll
+  for (int f = 0; f < Nf; ++f) U[f] = Qs[id + f * Nq];
+  adj::VU_vjp<DIM>(U, x, gas_of(P), Ub);
+#pragma unroll
+  for (int f = 0; f < Nf; ++f) {
+    const double qb = Qbar[id + f * Nq];
+    const double rt = fma(b, qb, resbar[id + f * Nq]);
+    resbar[id + f * Nq] = a * rt;
+    Qbar[id + f * Nq] = qb + Ub[f];
+  }
+}
+
+}  // namespace wadg
