@@ -42,6 +42,8 @@ struct wadg_adjoint {
   double *Qbar = nullptr, *resbar = nullptr, *rhsbar = nullptr, *sfbar = nullptr;
   double *vbar = nullptr, *vfbar = nullptr;
   double *sQ = nullptr, *sR = nullptr, *suq = nullptr, *suf = nullptr, *srhsQf = nullptr;
+  // transposes of the operators the adjoint applies transposed (column-major)
+  double *VqPqT = nullptr, *VfPqT = nullptr, *VqLqT = nullptr;
 };
 
 namespace {
@@ -99,7 +101,7 @@ int launch_seed(const wadg_adjoint *j, double b, double dt) {
   auto kern = adj_seed_kernel<DIM, N, CURVED, E>;
   static bool attr = false;
   if (int r = set_smem(kern, C::smem, attr, "adjoint seed kernel smem attribute")) return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, a->stream>>>(a->K, a->Jq, a->VqPq, a->VqLq, b, dt,
+  kern<<<(a->K + E - 1) / E, C::threads, C::smem, a->stream>>>(a->K, a->Jq, j->VqPqT, j->VqLqT, b, dt,
                                                               j->Qbar, j->resbar, j->rhsbar,
                                                               j->sfbar);
   return ck(cudaGetLastError(), "adjoint seed kernel");
@@ -132,7 +134,7 @@ int launch_proj(const wadg_adjoint *j, const double *Qs, double ra, double rb) {
   auto kern = adj_proj_kernel<DIM, N, CURVED, E>;
   static bool attr = false;
   if (int r = set_smem(kern, C::smem, attr, "adjoint projection kernel smem attribute")) return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, a->stream>>>(a->K, a->Jq, a->VqPq, a->VfPq, Qs,
+  kern<<<(a->K + E - 1) / E, C::threads, C::smem, a->stream>>>(a->K, a->Jq, j->VqPqT, j->VfPqT, Qs,
                                                               j->vbar, j->vfbar, ra, rb, j->Qbar,
                                                               j->resbar, j->phys);
   return ck(cudaGetLastError(), "adjoint projection kernel");
@@ -209,8 +211,9 @@ int d2d(double *dst, const double *src, size_t n, cudaStream_t s) {
 }
 
 void free_adj(wadg_adjoint *j) {
-  double *bufs[] = {j->ckpt, j->tapeQ, j->tapeU, j->tapeUf, j->Qbar, j->resbar, j->rhsbar,
-                    j->sfbar, j->vbar, j->vfbar, j->sQ, j->sR, j->suq, j->suf, j->srhsQf};
+  double *bufs[] = {j->ckpt,   j->tapeQ, j->tapeU, j->tapeUf,  j->Qbar,  j->resbar,
+                    j->rhsbar, j->sfbar, j->vbar,  j->vfbar,   j->sQ,    j->sR,
+                    j->suq,    j->suf,   j->srhsQf, j->VqPqT, j->VfPqT, j->VqLqT};
   for (double *b : bufs)
     if (b) cudaFree(b);
 }
@@ -265,6 +268,28 @@ int wadg_adjoint_create(wadg_app *app, int nsteps, int every, wadg_adjoint **out
       free_adj(j);
       delete j;
       return jfail(WADG_ERR_CUDA, "cudaMalloc (adjoint tape)", e);
+    }
+  }
+  // transposed operators: one host round trip at creation
+  {
+    const int Nq = app->Nq, NF = app->NfqNf;
+    struct {
+      const double *src;
+      double **dst;
+      int rows, cols;
+    } tr[] = {{app->VqPq, &j->VqPqT, Nq, Nq}, {app->VfPq, &j->VfPqT, NF, Nq}, {app->VqLq, &j->VqLqT, Nq, NF}};
+    for (auto &x : tr) {
+      std::vector<double> A((size_t)x.rows * x.cols), B(A.size());
+      cudaError_t e = cudaMemcpy(A.data(), x.src, A.size() * sizeof(double), cudaMemcpyDeviceToHost);
+      for (int c = 0; c < x.cols && e == cudaSuccess; ++c)
+        for (int r = 0; r < x.rows; ++r) B[c + (size_t)r * x.cols] = A[r + (size_t)c * x.rows];
+      if (e == cudaSuccess) e = cudaMalloc((void **)x.dst, B.size() * sizeof(double));
+      if (e == cudaSuccess) e = cudaMemcpy(*x.dst, B.data(), B.size() * sizeof(double), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        free_adj(j);
+        delete j;
+        return jfail(WADG_ERR_CUDA, "transposed operators", e);
+      }
     }
   }
   *out = j;

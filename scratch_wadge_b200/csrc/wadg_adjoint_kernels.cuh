@@ -63,7 +63,9 @@ __device__ __forceinline__ void polyG_d(double u, double &G, double &dG) {
 
 // Vector-Jacobian product of the contracted two-point flux F_S(a, b).n
 // (ecflux_n; Euler3Daffine.okl:107-148, Euler2D.okl:139-161) with the
-// adjoint c of its Nfields components.  Adds the adjoints of a's and b's
+// adjoint c of its Nfields components, split into the part that depends on
+// the two states only (FluxCore: the means and their partial derivatives)
+// and a reverse sweep per (n, c) that adds the adjoints of a's and b's
 // primitive states (rho, velocity, beta) to ba and bb.
 //
 // Log-mean derivatives (L(a,b) = (a-b)/(log a - log b), s = a+b, f = (a-b)/s,
@@ -74,75 +76,160 @@ __device__ __forceinline__ void polyG_d(double u, double &G, double &dG) {
 //   log form:    d(1/L)/da = (1/a - 1/L)/(a-b), d(1/L)/db = (1/L - 1/b)/(a-b)
 //   series form: d(1/L)/da = 2/s^2 (-F + 2F' f(1-f)), d(1/L)/db = 2/s^2 (-F - 2F' f(1+f))
 // with the same branch switch (u < 1e-2) as the forward flux.
-template <int DIM>
-__device__ __forceinline__ void ecflux_vjp(const AdjNode<DIM> &a, const AdjNode<DIM> &b,
-                                           const double *n, const double *c, const Phys &P,
-                                           double *ba, double *bb) {
+template <int DIM> struct FluxCore {
+  double rl, rla, rlb, ibl, ibla, iblb, pa, isb, ubar[DIM], vv;
+};
+
+__device__ __forceinline__ void rl_series(double sr, double fr, double G, double dG, double &rl,
+                                          double &rla, double &rlb) {
+  rl = 0.5 * sr * G;
+  const double t = dG * fr;
+  rla = fma(-t, fr, fma(0.5, G, t));
+  rlb = fma(-t, fr, fma(0.5, G, -t));
+}
+__device__ __forceinline__ void ibl_series(double isb, double fb, double F, double dF,
+                                           double &ibl, double &ibla, double &iblb) {
+  ibl = 2.0 * isb * F;
+  const double t2 = 2.0 * isb * isb, t = 2.0 * dF * fb;
+  ibla = t2 * (fma(-t, fb, t) - F);
+  iblb = t2 * (fma(-t, fb, -t) - F);
+}
+
+// WARP = true: must be called by all 32 lanes of a converged warp; when every
+// lane has u < 1e-6 for both means (nearly equal states, e.g. the whole
+// Taylor-Green field) the series are truncated at u^2 (remainders below
+// 1e-18 relative in the means and 1e-13 in their u-derivatives, which enter
+// multiplied by f < 1e-3)
+template <int DIM, bool WARP>
+__device__ __forceinline__ FluxCore<DIM> flux_core(const AdjNode<DIM> &a, const AdjNode<DIM> &b) {
+  FluxCore<DIM> k;
   const double sr = a.rho + b.rho, dr = a.rho - b.rho;
   const double sb = a.beta + b.beta, db = a.beta - b.beta;
-  const double isr = rcp(sr), isb = rcp(sb);
-  const double fr = dr * isr, fb = db * isb;
+  const double isr = rcp(sr);
+  k.isb = rcp(sb);
+  const double fr = dr * isr, fb = db * k.isb;
   const double ur = fr * fr, ub = fb * fb;
-  double rl, rla, rlb, ibl, ibla, iblb;
-  if (ur < 1e-2) {
-    double G, dG;
-    polyG_d(ur, G, dG);
-    rl = 0.5 * sr * G;
-    const double t = dG * fr;
-    rla = fma(-t, fr, fma(0.5, G, t));
-    rlb = fma(-t, fr, fma(0.5, G, -t));
+  if (WARP && __all_sync(0xffffffffu, fmax(ur, ub) < 1e-6)) {
+    rl_series(sr, fr, fma(fma(ur, -4.0 / 45.0, -1.0 / 3.0), ur, 1.0), fma(ur, -8.0 / 45.0, -1.0 / 3.0),
+              k.rl, k.rla, k.rlb);
+    ibl_series(k.isb, fb, fma(fma(ub, 1.0 / 5.0, 1.0 / 3.0), ub, 1.0), fma(ub, 2.0 / 5.0, 1.0 / 3.0),
+               k.ibl, k.ibla, k.iblb);
   } else {
-    const double ild = rcp(a.lrho - b.lrho);
-    rl = dr * ild;
-    rla = fma(-rl, a.irho, 1.0) * ild;
-    rlb = fma(rl, b.irho, -1.0) * ild;
+    if (ur < 1e-2) {
+      double G, dG;
+      polyG_d(ur, G, dG);
+      rl_series(sr, fr, G, dG, k.rl, k.rla, k.rlb);
+    } else {
+      const double ild = rcp(a.lrho - b.lrho);
+      k.rl = dr * ild;
+      k.rla = fma(-k.rl, a.irho, 1.0) * ild;
+      k.rlb = fma(k.rl, b.irho, -1.0) * ild;
+    }
+    if (ub < 1e-2) {
+      double F, dF;
+      polyF_d(ub, F, dF);
+      ibl_series(k.isb, fb, F, dF, k.ibl, k.ibla, k.iblb);
+    } else {
+      const double idb = rcp(db);
+      k.ibl = (a.lbeta - b.lbeta) * idb;
+      k.ibla = (a.ibeta - k.ibl) * idb;
+      k.iblb = (k.ibl - b.ibeta) * idb;
+    }
   }
-  if (ub < 1e-2) {
-    double F, dF;
-    polyF_d(ub, F, dF);
-    ibl = 2.0 * isb * F;
-    const double t2 = 2.0 * isb * isb, t = 2.0 * dF * fb;
-    ibla = t2 * (fma(-t, fb, t) - F);
-    iblb = t2 * (fma(-t, fb, -t) - F);
-  } else {
-    const double idb = rcp(db);
-    ibl = (a.lbeta - b.lbeta) * idb;
-    ibla = (a.ibeta - ibl) * idb;
-    iblb = (ibl - b.ibeta) * idb;
-  }
-  const double pa = 0.5 * sr * isb;
-  double ubar[DIM], un = 0.0, vv = 0.0, cu = 0.0, cn = 0.0;
+  k.pa = 0.5 * sr * k.isb;
+  k.vv = 0.0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    ubar[d] = 0.5 * (a.vel[d] + b.vel[d]);
-    un = fma(ubar[d], n[d], un);
-    vv = fma(a.vel[d], b.vel[d], vv);
-    cu = fma(c[1 + d], ubar[d], cu);
+    k.ubar[d] = 0.5 * (a.vel[d] + b.vel[d]);
+    k.vv = fma(a.vel[d], b.vel[d], k.vv);
+  }
+  return k;
+}
+
+// reverse sweep for one direction n and adjoint c; BSIDE = false skips b's adjoint
+template <int DIM, bool BSIDE>
+__device__ __forceinline__ void flux_rev(const FluxCore<DIM> &k, const AdjNode<DIM> &a,
+                                         const AdjNode<DIM> &b, const double *n, const double *c,
+                                         const Phys &P, double *ba, double *bb) {
+  double un = 0.0, cu = 0.0, cn = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    un = fma(k.ubar[d], n[d], un);
+    cu = fma(c[1 + d], k.ubar[d], cu);
     cn = fma(c[1 + d], n[d], cn);
   }
-  const double h = fma(ibl, P.cbeta, 0.5 * vv);
-  const double f4 = fma(rl, h, pa);
-  const double F0 = rl * un;
+  const double h = fma(k.ibl, P.cbeta, 0.5 * k.vv);
+  const double f4 = fma(k.rl, h, k.pa);
+  const double F0 = k.rl * un;
   const double cE = c[DIM + 1];
-  // reverse sweep
   const double F0b = c[0] + cu;
   const double f4b = cE * un;
-  const double unb = fma(F0b, rl, cE * f4);
+  const double unb = fma(F0b, k.rl, cE * f4);
   const double rlbar = fma(F0b, un, f4b * h);
-  const double iblbar = f4b * rl * P.cbeta;
-  const double vvb = 0.5 * f4b * rl;
+  const double iblbar = f4b * k.rl * P.cbeta;
+  const double vvb = 0.5 * f4b * k.rl;
   const double pab = cn + f4b;
-  const double prho = 0.5 * pab * isb, pbeta = -pab * pa * isb;
-  ba[0] = fma(rlbar, rla, ba[0] + prho);
-  bb[0] = fma(rlbar, rlb, bb[0] + prho);
-  ba[DIM + 1] = fma(iblbar, ibla, ba[DIM + 1] + pbeta);
-  bb[DIM + 1] = fma(iblbar, iblb, bb[DIM + 1] + pbeta);
+  const double prho = 0.5 * pab * k.isb, pbeta = -pab * k.pa * k.isb;
+  ba[0] = fma(rlbar, k.rla, ba[0] + prho);
+  ba[DIM + 1] = fma(iblbar, k.ibla, ba[DIM + 1] + pbeta);
+  if (BSIDE) {
+    bb[0] = fma(rlbar, k.rlb, bb[0] + prho);
+    bb[DIM + 1] = fma(iblbar, k.iblb, bb[DIM + 1] + pbeta);
+  }
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
     const double hb = 0.5 * fma(c[1 + d], F0, unb * n[d]);
     ba[1 + d] = fma(vvb, b.vel[d], ba[1 + d] + hb);
-    bb[1 + d] = fma(vvb, a.vel[d], bb[1 + d] + hb);
+    if (BSIDE) bb[1 + d] = fma(vvb, a.vel[d], bb[1 + d] + hb);
   }
+}
+
+template <int DIM, bool WARP>
+__device__ __forceinline__ void ecflux_vjp(const AdjNode<DIM> &a, const AdjNode<DIM> &b,
+                                           const double *n, const double *c, const Phys &P,
+                                           double *ba, double *bb) {
+  const FluxCore<DIM> k = flux_core<DIM, WARP>(a, b);
+  flux_rev<DIM, true>(k, a, b, n, c, P, ba, bb);
+}
+
+// adjoint of the primitive recovery (rho, u = m/rho, beta = rho/(2p)) at a
+// node: primitive adjoint pb -> conservative adjoint Ub; with p = rho/(2 beta),
+// d beta/d(rho, m, E) = -2 beta^2/rho * dp/d(.) + (beta/rho, 0, 0)
+template <int DIM>
+__device__ __forceinline__ void prim_vjp_dev(const AdjNode<DIM> &s, const double *pb,
+                                             const Phys &P, double *Ub) {
+  double kin = 0.0, pu = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    kin = fma(s.vel[d], s.vel[d], kin);
+    pu = fma(pb[1 + d], s.vel[d], pu);
+  }
+  const double q = -2.0 * s.beta * s.beta * s.irho * pb[DIM + 1];  // beta-bar * d beta / dp
+  Ub[0] = pb[0] + pb[DIM + 1] * s.beta * s.irho + q * P.gm1 * 0.5 * kin - pu * s.irho;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) Ub[1 + d] = fma(pb[1 + d], s.irho, -q * P.gm1 * s.vel[d]);
+  Ub[DIM + 1] = q * P.gm1;
+}
+
+// wave speed lambda = |u| + sqrt(gamma p / rho) = |u| + sqrt(gamma / (2 beta))
+// and (GRAD) its gradient with respect to the conservative state
+template <int DIM, bool GRAD>
+__device__ __forceinline__ double lambda_dev(const AdjNode<DIM> &s, const Phys &P, double *dl) {
+  double kin = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) kin = fma(s.vel[d], s.vel[d], kin);
+  const double un = sqrt(kin), c = sqrt(0.5 * P.gamma * s.ibeta);
+  if (GRAD) {
+    // d|u|/drho = -|u|/rho, d|u|/dm = u/(|u| rho); dc = gamma/(2c) (dp/rho - p/rho^2)
+    const double k = 0.5 * P.gamma * rcp(c) * s.irho;
+    const double iun = un > 0.0 ? rcp(un) : 0.0;
+    const double p_over_rho = 0.5 * s.ibeta;
+    dl[0] = fma(k, fma(P.gm1 * 0.5, kin, -p_over_rho), -un * s.irho);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) dl[1 + d] = s.vel[d] * s.irho * fma(-k, P.gm1 * s.rho, iun);
+    dl[DIM + 1] = k * P.gm1;
+  }
+  return un + c;
 }
 
 template <int DIM>
@@ -176,8 +263,8 @@ template <int DIM, int N, int E> struct AdjSeedCfg {
 
 template <int DIM, int N, bool CURVED, int E>
 __global__ void __launch_bounds__(AdjSeedCfg<DIM, N, E>::threads)
-adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
-                const double *__restrict__ VqLq, double b, double dt,
+adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
+                const double *__restrict__ VqLqT, double b, double dt,
                 const double *__restrict__ Qbar, const double *__restrict__ resbar,
                 double *__restrict__ rhsbar, double *__restrict__ sfbar) {
   using El = Elem<DIM, N>;
@@ -192,12 +279,13 @@ adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
   const size_t id = (size_t)k * Nq * Nf + i;
   const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
 
-  // transposed matvec: out[f] = sum_j Op(j, row) X[f][j]  (Op column-major, ld rows)
-  auto matvecT = [&](const double *Op, int ld, int row, double (*X)[Nq], double *out) {
+  // transposed matvec from the stored transpose: out[f] = sum_j OpT(row, j) X[f][j]
+  // (OpT column-major with ld rows; consecutive threads read consecutive rows)
+  auto matvecT = [&](const double *OpT, int ld, int row, double (*X)[Nq], double *out) {
 #pragma unroll
     for (int f = 0; f < Nf; ++f) out[f] = 0.0;
     for (int j = 0; j < Nq; ++j) {
-      const double w = __ldg(Op + j + row * ld);
+      const double w = __ldg(OpT + row + j * ld);
 #pragma unroll
       for (int f = 0; f < Nf; ++f) out[f] = fma(w, X[f][j], out[f]);
     }
@@ -214,15 +302,15 @@ adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
   double r[Nf];
   if (CURVED) {
     if (valid) {
-      matvecT(VqPq, Nq, i, sA[e], r);
+      matvecT(VqPqT, Nq, i, sA[e], r);
 #pragma unroll
       for (int f = 0; f < Nf; ++f) sB[e][f][i] = -2.0 * r[f] / Jqi;
     }
     __syncthreads();
-    if (valid) matvecT(VqPq, Nq, i, sB[e], r);
+    if (valid) matvecT(VqPqT, Nq, i, sB[e], r);
     __syncthreads();
   } else if (valid) {
-    matvecT(VqPq, Nq, i, sA[e], r);
+    matvecT(VqPqT, Nq, i, sA[e], r);
   }
   if (valid) {
 #pragma unroll
@@ -236,7 +324,7 @@ adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
   for (int t = threadIdx.x; t < kend * NF; t += blockDim.x) {
     const int ee = t / NF, fn = t % NF;
     double s[Nf];
-    matvecT(VqLq, Nq, fn, sB[ee], s);
+    matvecT(VqLqT, NF, fn, sB[ee], s);
     double *out = sfbar + (size_t)(k0 + ee) * NF * Nf + fn;
 #pragma unroll
     for (int f = 0; f < Nf; ++f) out[f * NF] = s[f];
@@ -473,7 +561,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
             }
             nvd[d] = v;
           }
-          ecflux_vjp<DIM>(A[r], B, nvd, cr[r], P, rb[r], cb);
+          ecflux_vjp<DIM, true>(A[r], B, nvd, cr[r], P, rb[r], cb);
         }
 #pragma unroll
         for (int q = 0; q < NB; ++q) bar[q * NN + j] += cb[q];
@@ -518,7 +606,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           double c[Nf];
 #pragma unroll
           for (int q = 0; q < Nf; ++q) c[q] = fma(w1, cr[r][q], w2 * cfs[q]);
-          ecflux_vjp<DIM>(A[r], B, nvd, c, P, rb[r], cb);
+          ecflux_vjp<DIM, true>(A[r], B, nvd, c, P, rb[r], cb);
         }
 #pragma unroll
         for (int q = 0; q < NB; ++q) bar[q * NN + Nq + f] += cb[q];
@@ -546,23 +634,33 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     for (int t = tid; t < E * NN; t += blockDim.x) {
       const int ee = t / NN, n = t % NN, k = k0 + ee;
       if (k >= K) continue;
-      const double *bt = sEl + ee * C::per_elem + C::SST + C::SSF;
-      adj::PrimBar<DIM> pb;
-      pb.rho = bt[n];
+      const double *ste = sEl + ee * C::per_elem;
+      const double *bt = ste + C::SST + C::SSF;
+      AdjNode<DIM> own;
+      own.rho = ste[n];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) pb.u[d] = bt[(1 + d) * NN + n];
-      pb.beta = bt[(DIM + 1) * NN + n];
-      double U[Nf], Ub[Nf], Vv[Nf], Vb[Nf];
+      for (int d = 0; d < DIM; ++d) own.vel[d] = ste[(1 + d) * NN + n];
+      own.beta = ste[(DIM + 1) * NN + n];
+      own.lrho = ste[(DIM + 2) * NN + n];
+      own.lbeta = ste[(DIM + 3) * NN + n];
+      own.irho = ste[(DIM + 4) * NN + n];
+      own.ibeta = ste[(DIM + 5) * NN + n];
+      double pb[NB], U[Nf], Ub[Nf], Vb[Nf];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) pb[q] = bt[q * NN + n];
       if (n < Nq) {
-        const double *q = uq + (size_t)k * Nq * Nf + n;
+        const double *qv = uq + (size_t)k * Nq * Nf + n;
 #pragma unroll
-        for (int f = 0; f < Nf; ++f) U[f] = q[f * Nq];
-        adj::prim_vjp<DIM>(U, pb, gas, Ub);
+        for (int f = 0; f < Nf; ++f) U[f] = qv[f * Nq];
+        prim_vjp_dev<DIM>(own, pb, P, Ub);
       } else {
         // surface flux + Lax-Friedrichs penalty (Euler3Daffine.okl:421-552,
         // Euler3D.okl:3242-3473, Euler2D.okl:1357-1495):
-        //   sf_j = 1/2 F_S(u_j, u_P).nJ_j - tau/4 max(lam_j, lam_P) sJ_j (u_P - u_j)
-        // own evaluation (j as the minus side) and the neighbour's (j as its plus side)
+        //   sf_j = 1/2 F_S(u_j, u_P).nJ_j - tau/4 max(lam_j, lam_P) sJ_j (u_P - u_j).
+        // Face point j enters its own evaluation (as the minus side) and its
+        // neighbour m's (as the plus side); the flux is symmetric in its two
+        // states, so both are the a-side adjoint of one F_S(u_j, u_m) with
+        // the two (direction, seed) pairs (nJ_j/2, sfbar_j) and (nJ_m/2, sfbar_m).
         const int j = n - Nq;
         const size_t idM = (size_t)k * NF * Nf + j;
         const size_t idP = mapPq[(size_t)k * NF + j];
@@ -572,7 +670,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
         for (int f = 0; f < Nf; ++f) {
           U[f] = uf[idM + f * NF];
           UP[f] = uf[idP + f * NF];
-          cM[f] = bt[-C::SSF + f * NF + j];  // this element's sfbar, staged in shared memory
+          cM[f] = ste[C::SST + f * NF + j];  // this element's sfbar, staged in shared memory
           cP[f] = sfbar[idP + f * NF];
         }
         const double *fgM = fgeo + (size_t)k * NF * NFG + j;
@@ -583,33 +681,32 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           nP[d] = 0.5 * fgP[d * NF];
         }
         const double sJM = fgM[DIM * NF], sJP = fgP[DIM * NF];
-        const adj::Prim<DIM> pM = adj::prim<DIM>(U, gas), pP = adj::prim<DIM>(UP, gas);
-        adj::PrimBar<DIM> dummy;
-        adj::zero(dummy);
-        adj::flux_vjp<DIM>(pM, pP, nM, gas, cM, pb, dummy);  // own: j is a
-        adj::flux_vjp<DIM>(pP, pM, nP, gas, cP, dummy, pb);  // neighbour's: j is b
-        adj::prim_vjp<DIM>(U, pb, gas, Ub);
-        double dlM[Nf], dlP[Nf];
-        const double lamM = adj::lambda_d<DIM>(U, gas, dlM);
-        const double lamP = adj::lambda_d<DIM>(UP, gas, dlP);
+        const AdjNode<DIM> nb = adj_node<DIM>(UP, 1, P);
+        const FluxCore<DIM> core = flux_core<DIM, false>(own, nb);
+        flux_rev<DIM, false>(core, own, nb, nM, cM, P, pb, nullptr);
+        flux_rev<DIM, false>(core, own, nb, nP, cP, P, pb, nullptr);
+        prim_vjp_dev<DIM>(own, pb, P, Ub);
+        double dl[Nf];
+        const double lamM = lambda_dev<DIM, true>(own, P, dl);
+        const double lamP = lambda_dev<DIM, false>(nb, P, nullptr);
         const double tq = (DIM == 3 ? P.tau : 1.0) * 0.25;
         const double lmax = fmax(lamM, lamP);
         double LbM = 0.0, LbP = 0.0;
 #pragma unroll
         for (int f = 0; f < Nf; ++f) {
           const double du = UP[f] - U[f];
-          Ub[f] += tq * lmax * (sJM * cM[f] - sJP * cP[f]);
-          LbM -= cM[f] * du;   // adjoint of the own penalty scale
-          LbP += cP[f] * du;   // ... and of the neighbour's (its jump is u_j - u_P)
+          Ub[f] = fma(tq * lmax, sJM * cM[f] - sJP * cP[f], Ub[f]);
+          LbM = fma(-cM[f], du, LbM);  // adjoint of the own penalty scale
+          LbP = fma(cP[f], du, LbP);   // ... and of the neighbour's (its jump is u_j - u_P)
         }
-        // the max takes the branch the forward took: own lam_j > lam_P picks j;
-        // at the neighbour, lam_P > lam_j picks the neighbour, otherwise j
+        // the max takes the branch the forward took (`lamM > lamP ? lamM : lamP`):
+        // the own evaluation picks j when lam_j > lam_P; the neighbour's picks
+        // j unless lam_P > lam_j
         const double gsel = (lamM > lamP ? LbM * sJM : 0.0) + (lamP > lamM ? 0.0 : LbP * sJP);
 #pragma unroll
-        for (int f = 0; f < Nf; ++f) Ub[f] = fma(tq * gsel, dlM[f], Ub[f]);
+        for (int f = 0; f < Nf; ++f) Ub[f] = fma(tq * gsel, dl[f], Ub[f]);
       }
-      adj::V_of_U<DIM>(U, gas, Vv);
-      adj::UV_vjp<DIM>(Vv, Ub, gas, Vb);
+      adj::UV_vjp_U<DIM>(U, Ub, gas, Vb);
       if (n < Nq) {
         double *o = vbar + (size_t)k * Nq * Nf + n;
 #pragma unroll
@@ -637,8 +734,8 @@ template <int DIM, int N, int E> struct AdjProjCfg {
 
 template <int DIM, int N, bool CURVED, int E>
 __global__ void __launch_bounds__(AdjProjCfg<DIM, N, E>::threads)
-adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
-                const double *__restrict__ VfPq, const double *__restrict__ Qs,
+adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
+                const double *__restrict__ VfPqT, const double *__restrict__ Qs,
                 const double *__restrict__ vbar, const double *__restrict__ vfbar, double a,
                 double b, double *__restrict__ Qbar, double *__restrict__ resbar, Phys P) {
   using El = Elem<DIM, N>;
@@ -665,12 +762,12 @@ adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
   for (int f = 0; f < Nf; ++f) x[f] = 0.0;
   if (valid) {
     for (int j = 0; j < Nq; ++j) {
-      const double w = __ldg(VqPq + j + i * Nq);
+      const double w = __ldg(VqPqT + i + j * Nq);
 #pragma unroll
       for (int f = 0; f < Nf; ++f) x[f] = fma(w, sV[e][f][j], x[f]);
     }
     for (int j = 0; j < NF; ++j) {
-      const double w = __ldg(VfPq + j + i * NF);
+      const double w = __ldg(VfPqT + i + j * Nq);
 #pragma unroll
       for (int f = 0; f < Nf; ++f) x[f] = fma(w, sVf[e][f][j], x[f]);
     }
@@ -686,7 +783,7 @@ adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
     for (int f = 0; f < Nf; ++f) y[f] = 0.0;
     if (valid) {
       for (int j = 0; j < Nq; ++j) {
-        const double w = __ldg(VqPq + j + i * Nq);
+        const double w = __ldg(VqPqT + i + j * Nq);
 #pragma unroll
         for (int f = 0; f < Nf; ++f) y[f] = fma(w, sX[e][f][j], y[f]);
       }
@@ -698,7 +795,7 @@ adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
 #pragma unroll
       for (int f = 0; f < Nf; ++f) x[f] = 0.0;
       for (int j = 0; j < Nq; ++j) {
-        const double w = __ldg(VqPq + j + i * Nq);
+        const double w = __ldg(VqPqT + i + j * Nq);
 #pragma unroll
         for (int f = 0; f < Nf; ++f) x[f] = fma(w, sV[e][f][j], x[f]);
       }

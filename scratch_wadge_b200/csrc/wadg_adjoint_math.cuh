@@ -208,6 +208,28 @@ WADG_HD void UV_vjp(const double *V, const double *Ub, const Gas &g, double *Vb)
                 Ub[DIM + 1] * rhoe * vv / (2.0 * Vl * Vl);
 }
 
+// adjoint of U(V) at V = V(U), written in terms of U (no exp or log):
+// with rhoe = E - |m|^2/(2 rho), u = m/rho, V_m = m/rhoe, V_l = -rho/rhoe,
+// -V_m/V_l = u, 1/V_l = -rhoe/rho and |V_m|^2/(2 V_l^2) = |u|^2/2
+template <int DIM>
+WADG_HD void UV_vjp_U(const double *U, const double *Ub, const Gas &g, double *Vb) {
+  const double rho = U[0], ir = 1.0 / rho;
+  double u[DIM], u2 = 0.0;
+  for (int d = 0; d < DIM; ++d) {
+    u[d] = U[1 + d] * ir;
+    u2 += u[d] * u[d];
+  }
+  const double rhoe = U[DIM + 1] - 0.5 * rho * u2;
+  const double irhoe = 1.0 / rhoe;
+  // rb = Ub . dU/d(rhoe) = Ub0 rho/rhoe + Ub_m m/rhoe + UbE (1 + rho |u|^2 / (2 rhoe))
+  double rb = Ub[0] * rho * irhoe + Ub[DIM + 1] * (1.0 + 0.5 * rho * u2 * irhoe);
+  for (int d = 0; d < DIM; ++d) rb += Ub[1 + d] * U[1 + d] * irhoe;
+  const double t = rb * rhoe * g.igm1;  // adjoint of the exponent, over (gamma - 1)
+  Vb[0] = t;
+  for (int d = 0; d < DIM; ++d) Vb[1 + d] = t * u[d] + (Ub[1 + d] + Ub[DIM + 1] * u[d]) * rhoe;
+  Vb[DIM + 1] = t * (g.gamma * rhoe * ir + 0.5 * u2) + (Ub[DIM + 1] * 0.5 * u2 - Ub[0]) * rhoe;
+}
+
 // adjoint of V(U): Vb -> Ub  (U at which V is evaluated)
 template <int DIM>
 WADG_HD void VU_vjp(const double *U, const double *Vb, const Gas &g, double *Ub) {

@@ -47,4 +47,7 @@ void am_VU_vjp(int dim, const double *U, const double *Vb, double g, double *Ub)
 void am_UV_vjp(int dim, const double *V, const double *Ub, double g, double *Vb) {
   dim == 3 ? UV_vjp<3>(V, Ub, gas(g), Vb) : UV_vjp<2>(V, Ub, gas(g), Vb);
 }
+void am_UV_vjp_U(int dim, const double *U, const double *Ub, double g, double *Vb) {
+  dim == 3 ? UV_vjp_U<3>(U, Ub, gas(g), Vb) : UV_vjp_U<2>(U, Ub, gas(g), Vb);
+}
 }

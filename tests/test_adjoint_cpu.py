@@ -37,7 +37,8 @@ def am():
                                SHIM, "-o", SO])
     L = ctypes.CDLL(SO)
     L.am_lambda.restype = ctypes.c_double
-    for f in ("am_flux", "am_flux_vjp", "am_lambda", "am_VU", "am_UV", "am_VU_vjp", "am_UV_vjp"):
+    for f in ("am_flux", "am_flux_vjp", "am_lambda", "am_VU", "am_UV", "am_VU_vjp", "am_UV_vjp",
+              "am_UV_vjp_U"):
         getattr(L, f).argtypes = None
     return L
 
@@ -104,6 +105,8 @@ def test_node_map_vjps_against_central_differences(am, dim):
         V = _call(am.am_VU, dim, U, G)[0]
         gV = _call(am.am_UV_vjp, dim, V, Ub, G)[0]
         assert rel(_call(am.am_UV, dim, V, G)[0], U) < 1e-13
+        # the kernels' form of the U(V) adjoint, written in terms of U = U(V)
+        assert rel(_call(am.am_UV_vjp_U, dim, U, Ub, G)[0], gV) < 1e-13
         for i in range(dim + 2):
             h = 1e-6 * abs(U[i]) + 1e-9
             e = np.zeros(dim + 2)
@@ -138,7 +141,9 @@ def test_torch_autodiff_against_central_differences_of_oracle(name):
     _, vjp = torch.func.vjp(T.R, torch.from_numpy(Q))
     g = vjp(torch.from_numpy(w))[0].numpy()
     P = Port(c.ops, c.curved)
-    h = 1e-6
+    # step small enough that no face point's penalty max changes side within +-h
+    h = 1e-7
+    assert torch.equal(T.lf_branch(torch.from_numpy(Q + h * d)), T.lf_branch(torch.from_numpy(Q - h * d)))
     fd = (P.rhs(c.geo, Q + h * d) - P.rhs(c.geo, Q - h * d)) / (2 * h)
     a, b = float(np.sum(w * fd)), float(np.sum(g * d))
     assert abs(a - b) <= 1e-6 * abs(b)
