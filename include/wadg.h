@@ -291,8 +291,10 @@ int wadg_rk_stage_noalloc(wadg_ctx *ctx, int K, int curved, const double *vgeo,
  * creation. */
 typedef struct wadg_adjoint wadg_adjoint;
 /* Tape for `nsteps` time steps with a checkpoint every `every` steps:
- * device memory (nsteps/every + 1) Q-sized checkpoints plus 5*every stages
- * of (Q, u~, uf~). */
+ * device memory (nsteps/every + 1) Q-sized checkpoints plus two tapes of
+ * 5*every stages of (Q, u~, uf~) (one when there is a single segment), and
+ * a second CUDA stream on which the stage adjoints run beside the segment
+ * recompute. */
 int wadg_adjoint_create(wadg_app *app, int nsteps, int every,
                         wadg_adjoint **out);
 int wadg_adjoint_destroy(wadg_adjoint *adj);

@@ -3,7 +3,10 @@
 // sweep walks the segments backwards, recomputes each segment's stages from
 // its checkpoint into a tape (Q and the projected traces u~, uf~ at the start
 // of every stage) and runs the stage adjoint kernels (wadg_adjoint_kernels.cuh)
-// over the tape in reverse order.
+// over the tape in reverse order.  Recompute and adjoint run on two streams
+// with two tapes, so that the adjoint of segment s overlaps the recompute of
+// segment s-1: the forward kernels fill the SMs the adjoint kernels leave
+// idle (the pair kernel's last wave, the small per-element kernels).
 //
 // The first LSRK coefficient a_0 is 0, so a time step does not depend on the
 // residual register left by the previous one: a checkpoint is Q alone.  The
@@ -38,7 +41,12 @@ struct wadg_adjoint {
   double dt = 0.0;
   bool have_forward = false;
   double *ckpt = nullptr;                                      // (nseg + 1) x nv
-  double *tapeQ = nullptr, *tapeU = nullptr, *tapeUf = nullptr;  // 5*every stages
+  // two tapes of 5*every stages: the VJP of one segment reads one while the
+  // recompute of the previous segment fills the other
+  double *tapeQ[2] = {nullptr, nullptr}, *tapeU[2] = {nullptr, nullptr},
+         *tapeUf[2] = {nullptr, nullptr};
+  cudaStream_t vs = nullptr;  // stream of the stage adjoint kernels
+  cudaEvent_t evR[2] = {nullptr, nullptr}, evV[2] = {nullptr, nullptr}, evJoin = nullptr;
   double *Qbar = nullptr, *resbar = nullptr, *rhsbar = nullptr, *sfbar = nullptr;
   double *vbar = nullptr, *vfbar = nullptr;
   double *sQ = nullptr, *sR = nullptr, *suq = nullptr, *suf = nullptr, *srhsQf = nullptr;
@@ -94,21 +102,21 @@ int set_smem(F kern, size_t bytes, bool &done, const char *what) {
 }
 
 template <int DIM, int N, bool CURVED>
-int launch_seed(const wadg_adjoint *j, double b, double dt) {
+int launch_seed(const wadg_adjoint *j, cudaStream_t s, double b, double dt) {
   const wadg_app *a = j->app;
   constexpr int E = pickE(256, Elem<DIM, N>::Nq);
   using C = AdjSeedCfg<DIM, N, E>;
   auto kern = adj_seed_kernel<DIM, N, CURVED, E>;
   static bool attr = false;
   if (int r = set_smem(kern, C::smem, attr, "adjoint seed kernel smem attribute")) return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, a->stream>>>(a->K, a->Jq, j->VqPqT, j->VqLqT, b, dt,
+  kern<<<(a->K + E - 1) / E, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VqLqT, b, dt,
                                                               j->Qbar, j->resbar, j->rhsbar,
                                                               j->sfbar);
   return ck(cudaGetLastError(), "adjoint seed kernel");
 }
 
 template <int DIM, int N, bool CURVED>
-int launch_pairs(const wadg_adjoint *j, const double *uq, const double *uf) {
+int launch_pairs(const wadg_adjoint *j, cudaStream_t s, const double *uq, const double *uf) {
   const wadg_app *a = j->app;
   constexpr int W = adjW<DIM, N, CURVED>();
   using C = AdjPairsCfg<DIM, N, CURVED, W>;
@@ -119,7 +127,7 @@ int launch_pairs(const wadg_adjoint *j, const double *uq, const double *uf) {
   const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
   const int batches = (a->K + C::E - 1) / C::E;
   const int grid = batches < num_sms_adj() * per_sm ? batches : num_sms_adj() * per_sm;
-  kern<<<grid, C::threads, C::smem, a->stream>>>(a->K, a->vgeo, a->vfgeo, a->fgeo, a->mapPq, a->nrJ,
+  kern<<<grid, C::threads, C::smem, s>>>(a->K, a->vgeo, a->vfgeo, a->fgeo, a->mapPq, a->nrJ,
                                                   a->nsJ, a->ntJ, a->Drq, a->Dsq, a->Dtq, a->VqLq,
                                                   a->VfPq, uq, uf, j->rhsbar, j->sfbar, j->vbar,
                                                   j->vfbar, j->phys);
@@ -127,38 +135,38 @@ int launch_pairs(const wadg_adjoint *j, const double *uq, const double *uf) {
 }
 
 template <int DIM, int N, bool CURVED>
-int launch_proj(const wadg_adjoint *j, const double *Qs, double ra, double rb) {
+int launch_proj(const wadg_adjoint *j, cudaStream_t s, const double *Qs, double ra, double rb) {
   const wadg_app *a = j->app;
   constexpr int E = pickE(256, Elem<DIM, N>::Nq);
   using C = AdjProjCfg<DIM, N, E>;
   auto kern = adj_proj_kernel<DIM, N, CURVED, E>;
   static bool attr = false;
   if (int r = set_smem(kern, C::smem, attr, "adjoint projection kernel smem attribute")) return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, a->stream>>>(a->K, a->Jq, j->VqPqT, j->VfPqT, Qs,
+  kern<<<(a->K + E - 1) / E, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VfPqT, Qs,
                                                               j->vbar, j->vfbar, ra, rb, j->Qbar,
                                                               j->resbar, j->phys);
   return ck(cudaGetLastError(), "adjoint projection kernel");
 }
 
 template <int DIM, int N, bool CURVED>
-int stage_adjoint_t(const wadg_adjoint *j, const double *Qs, const double *uq, const double *uf,
-                    double ra, double rb, double dt) {
-  int r = launch_seed<DIM, N, CURVED>(j, rb, dt);
-  if (!r) r = launch_pairs<DIM, N, CURVED>(j, uq, uf);
-  if (!r) r = launch_proj<DIM, N, CURVED>(j, Qs, ra, rb);
+int stage_adjoint_t(const wadg_adjoint *j, cudaStream_t s, const double *Qs, const double *uq,
+                    const double *uf, double ra, double rb, double dt) {
+  int r = launch_seed<DIM, N, CURVED>(j, s, rb, dt);
+  if (!r) r = launch_pairs<DIM, N, CURVED>(j, s, uq, uf);
+  if (!r) r = launch_proj<DIM, N, CURVED>(j, s, Qs, ra, rb);
   return r;
 }
 
 // adjoint of one stage with coefficients (ra, rb, dt) at the taped state
-// (Qs, uq, uf): updates Qbar and resbar in place
-int stage_adjoint(const wadg_adjoint *j, const double *Qs, const double *uq, const double *uf,
-                  double ra, double rb, double dt) {
+// (Qs, uq, uf), on stream s: updates Qbar and resbar in place
+int stage_adjoint(const wadg_adjoint *j, cudaStream_t s, const double *Qs, const double *uq,
+                  const double *uf, double ra, double rb, double dt) {
   const wadg_app *a = j->app;
   const int dim = a->p.dim, N = a->p.N;
 #define WADG_ADJ_CASE(D_, N_)                                                           \
   if (dim == D_ && N == N_)                                                             \
-    return a->curved ? stage_adjoint_t<D_, N_, true>(j, Qs, uq, uf, ra, rb, dt)         \
-                     : stage_adjoint_t<D_, N_, false>(j, Qs, uq, uf, ra, rb, dt);
+    return a->curved ? stage_adjoint_t<D_, N_, true>(j, s, Qs, uq, uf, ra, rb, dt)      \
+                     : stage_adjoint_t<D_, N_, false>(j, s, Qs, uq, uf, ra, rb, dt);
   WADG_ADJ_CASE(2, 1) WADG_ADJ_CASE(2, 2) WADG_ADJ_CASE(2, 3) WADG_ADJ_CASE(2, 4)
   WADG_ADJ_CASE(3, 1) WADG_ADJ_CASE(3, 2) WADG_ADJ_CASE(3, 3) WADG_ADJ_CASE(3, 4)
 #undef WADG_ADJ_CASE
@@ -211,11 +219,38 @@ int d2d(double *dst, const double *src, size_t n, cudaStream_t s) {
 }
 
 void free_adj(wadg_adjoint *j) {
-  double *bufs[] = {j->ckpt,   j->tapeQ, j->tapeU, j->tapeUf,  j->Qbar,  j->resbar,
-                    j->rhsbar, j->sfbar, j->vbar,  j->vfbar,   j->sQ,    j->sR,
-                    j->suq,    j->suf,   j->srhsQf, j->VqPqT, j->VfPqT, j->VqLqT};
+  double *bufs[] = {j->ckpt,     j->tapeQ[0], j->tapeU[0], j->tapeUf[0], j->tapeQ[1],
+                    j->tapeU[1], j->tapeUf[1], j->Qbar,     j->resbar,    j->rhsbar,
+                    j->sfbar,    j->vbar,      j->vfbar,    j->sQ,        j->sR,
+                    j->suq,      j->suf,       j->srhsQf,   j->VqPqT,     j->VfPqT,
+                    j->VqLqT};
   for (double *b : bufs)
     if (b) cudaFree(b);
+  for (cudaEvent_t e : {j->evR[0], j->evR[1], j->evV[0], j->evV[1], j->evJoin})
+    if (e) cudaEventDestroy(e);
+  if (j->vs) cudaStreamDestroy(j->vs);
+}
+
+// recompute segment `seg` from its checkpoint on the app's stream, taping
+// (Q, u~, uf~) at the start of every stage into tape b
+int recompute(wadg_adjoint *j, int seg, int b) {
+  wadg_app *a = j->app;
+  cudaStream_t s = a->stream;
+  const int n = std::min(j->every, j->nsteps - seg * j->every);
+  int r;
+  if ((r = d2d(a->Q, j->ckpt + seg * j->nv, j->nv, s))) return r;
+  if ((r = project(a, a->Q, a->uq[a->cur], a->uf[a->cur], a->resQ))) return r;
+  for (int t = 0; t < n; ++t)
+    for (int st = 0; st < 5; ++st) {
+      const size_t idx = (size_t)t * 5 + st;
+      if ((r = d2d(j->tapeQ[b] + idx * j->nv, a->Q, j->nv, s)) ||
+          (r = d2d(j->tapeU[b] + idx * j->nv, a->uq[a->cur], j->nv, s)) ||
+          (r = d2d(j->tapeUf[b] + idx * j->nf, a->uf[a->cur], j->nf, s)))
+        return r;
+      if (t == n - 1 && st == 4) break;  // the last stage's outputs are not needed
+      if ((r = wadg_rk_step(a, RK4A[st], RK4B[st], j->dt))) return r;
+    }
+  return WADG_OK;
 }
 
 }  // namespace
@@ -254,15 +289,21 @@ int wadg_adjoint_create(wadg_app *app, int nsteps, int every, wadg_adjoint **out
   const double g = app->p.gamma;
   j->phys = Phys{g, g - 1.0, 1.0 / (2.0 * (g - 1.0)), app->p.tau, std::log(g - 1.0), 1.0 / (g - 1.0)};
   const size_t nst = (size_t)5 * (size_t)(every < nsteps ? every : (nsteps > 0 ? nsteps : 1));
+  const size_t nst2 = j->nseg > 1 ? nst : 0;  // the second tape only when there are two segments
   struct {
     double **p;
     size_t n;
-  } al[] = {{&j->ckpt, (j->nseg + 1) * j->nv}, {&j->tapeQ, nst * j->nv}, {&j->tapeU, nst * j->nv},
-            {&j->tapeUf, nst * j->nf},        {&j->Qbar, j->nv},        {&j->resbar, j->nv},
-            {&j->rhsbar, j->nv},              {&j->sfbar, j->nf},       {&j->vbar, j->nv},
-            {&j->vfbar, j->nf},               {&j->sQ, j->nv},          {&j->sR, j->nv},
-            {&j->suq, j->nv},                 {&j->suf, j->nf},         {&j->srhsQf, j->nf}};
+  } al[] = {{&j->ckpt, (j->nseg + 1) * j->nv}, {&j->tapeQ[0], nst * j->nv},
+            {&j->tapeU[0], nst * j->nv},        {&j->tapeUf[0], nst * j->nf},
+            {&j->tapeQ[1], nst2 * j->nv},       {&j->tapeU[1], nst2 * j->nv},
+            {&j->tapeUf[1], nst2 * j->nf},      {&j->Qbar, j->nv},
+            {&j->resbar, j->nv},                {&j->rhsbar, j->nv},
+            {&j->sfbar, j->nf},                 {&j->vbar, j->nv},
+            {&j->vfbar, j->nf},                 {&j->sQ, j->nv},
+            {&j->sR, j->nv},                    {&j->suq, j->nv},
+            {&j->suf, j->nf},                   {&j->srhsQf, j->nf}};
   for (auto &x : al) {
+    if (x.n == 0) continue;
     cudaError_t e = cudaMalloc((void **)x.p, x.n * sizeof(double));
     if (e != cudaSuccess) {
       free_adj(j);
@@ -290,6 +331,16 @@ int wadg_adjoint_create(wadg_app *app, int nsteps, int every, wadg_adjoint **out
         delete j;
         return jfail(WADG_ERR_CUDA, "transposed operators", e);
       }
+    }
+  }
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&j->vs, cudaStreamNonBlocking);
+    for (cudaEvent_t *ev : {&j->evR[0], &j->evR[1], &j->evV[0], &j->evV[1], &j->evJoin})
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      free_adj(j);
+      delete j;
+      return jfail(WADG_ERR_CUDA, "adjoint stream/events", e);
     }
   }
   *out = j;
@@ -328,38 +379,50 @@ int wadg_adjoint_reverse(wadg_adjoint *j, const double *QbarT, double *Qbar0) {
   if (!j || !QbarT || !Qbar0) return jfail(WADG_ERR_INVALID, "invalid argument");
   if (!j->have_forward) return jfail(WADG_ERR_INVALID, "wadg_adjoint_forward has not run");
   wadg_app *a = j->app;
-  cudaStream_t s = a->stream;
+  // two streams: the app's stream recomputes segments (forward kernels), the
+  // adjoint's stream runs the stage adjoints; segment seg's adjoint overlaps
+  // the recompute of segment seg-1 into the other tape
+  cudaStream_t sr = a->stream, sv = j->vs;
   const double dt = j->dt;
   int r;
-  if ((r = d2d(j->Qbar, QbarT, j->nv, s))) return r;
-  if ((r = ck(cudaMemsetAsync(j->resbar, 0, j->nv * sizeof(double), s), "memset"))) return r;
-  for (int seg = j->nseg - 1; seg >= 0; --seg) {
+  // the adjoint stream starts after what the caller queued on the app's stream
+  if ((r = ck(cudaEventRecord(j->evJoin, sr), "event")) ||
+      (r = ck(cudaStreamWaitEvent(sv, j->evJoin, 0), "event")))
+    return r;
+  if ((r = d2d(j->Qbar, QbarT, j->nv, sv))) return r;
+  if ((r = ck(cudaMemsetAsync(j->resbar, 0, j->nv * sizeof(double), sv), "memset"))) return r;
+  const int last = j->nseg - 1;
+  if (last >= 0) {
+    if ((r = recompute(j, last, last % 2))) return r;
+    if ((r = ck(cudaEventRecord(j->evR[last % 2], sr), "event"))) return r;
+  }
+  for (int seg = last; seg >= 0; --seg) {
+    const int b = seg % 2;
     const int n = std::min(j->every, j->nsteps - seg * j->every);
-    // recompute the segment from its checkpoint, taping every stage's input
-    if ((r = d2d(a->Q, j->ckpt + seg * j->nv, j->nv, s))) return r;
-    if ((r = project(a, a->Q, a->uq[a->cur], a->uf[a->cur], a->resQ))) return r;
-    for (int t = 0; t < n; ++t)
-      for (int st = 0; st < 5; ++st) {
-        const size_t idx = (size_t)t * 5 + st;
-        if ((r = d2d(j->tapeQ + idx * j->nv, a->Q, j->nv, s)) ||
-            (r = d2d(j->tapeU + idx * j->nv, a->uq[a->cur], j->nv, s)) ||
-            (r = d2d(j->tapeUf + idx * j->nf, a->uf[a->cur], j->nf, s)))
-          return r;
-        if (t == n - 1 && st == 4) break;  // the last stage's outputs are not needed
-        if ((r = wadg_rk_step(a, RK4A[st], RK4B[st], dt))) return r;
-      }
-    // stage adjoints in reverse order
+    if ((r = ck(cudaStreamWaitEvent(sv, j->evR[b], 0), "event"))) return r;
     for (int idx = n * 5 - 1; idx >= 0; --idx) {
       const int st = idx % 5;
-      if ((r = stage_adjoint(j, j->tapeQ + idx * j->nv, j->tapeU + idx * j->nv,
-                             j->tapeUf + idx * j->nf, RK4A[st], RK4B[st], dt)))
+      if ((r = stage_adjoint(j, sv, j->tapeQ[b] + idx * j->nv, j->tapeU[b] + idx * j->nv,
+                             j->tapeUf[b] + idx * j->nf, RK4A[st], RK4B[st], dt)))
         return r;
     }
+    if ((r = ck(cudaEventRecord(j->evV[b], sv), "event"))) return r;
+    if (seg > 0) {
+      const int nb = (seg - 1) % 2;  // the tape segment seg+1's adjoint read
+      if (seg < last && (r = ck(cudaStreamWaitEvent(sr, j->evV[nb], 0), "event"))) return r;
+      if ((r = recompute(j, seg - 1, nb))) return r;
+      if ((r = ck(cudaEventRecord(j->evR[nb], sr), "event"))) return r;
+    }
   }
-  if ((r = d2d(Qbar0, j->Qbar, j->nv, s))) return r;
-  // leave the app at the final state of the forward run
-  if ((r = d2d(a->Q, j->ckpt + j->nseg * j->nv, j->nv, s))) return r;
-  return project(a, a->Q, a->uq[a->cur], a->uf[a->cur], a->resQ);
+  if ((r = d2d(Qbar0, j->Qbar, j->nv, sv))) return r;
+  // leave the app at the final state of the forward run, and join the
+  // adjoint stream into the app's stream
+  if ((r = d2d(a->Q, j->ckpt + j->nseg * j->nv, j->nv, sr))) return r;
+  if ((r = project(a, a->Q, a->uq[a->cur], a->uf[a->cur], a->resQ))) return r;
+  if ((r = ck(cudaEventRecord(j->evJoin, sv), "event")) ||
+      (r = ck(cudaStreamWaitEvent(sr, j->evJoin, 0), "event")))
+    return r;
+  return WADG_OK;
 }
 
 int wadg_adjoint_rhs(wadg_adjoint *j, const double *Q, double *R) {
@@ -386,7 +449,7 @@ int wadg_adjoint_rhs_vjp(wadg_adjoint *j, const double *Q, const double *w, doub
   // (0, w) leaves Qbar = (dR/dQ)^T w
   if ((r = ck(cudaMemsetAsync(j->Qbar, 0, j->nv * sizeof(double), s), "memset"))) return r;
   if ((r = d2d(j->resbar, w, j->nv, s))) return r;
-  if ((r = stage_adjoint(j, j->sQ, j->suq, j->suf, 0.0, 0.0, 1.0))) return r;
+  if ((r = stage_adjoint(j, s, j->sQ, j->suq, j->suf, 0.0, 0.0, 1.0))) return r;
   return d2d(Qbar, j->Qbar, j->nv, s);
 }
 
