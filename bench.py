@@ -56,10 +56,8 @@ NHEX, N, CFL, E2E_STEPS = 16, 3, 0.5, 100
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from scratch_wadge_b200 import replicas as RP
+    return RP.env()
 
 
 def build_workload():
@@ -196,14 +194,10 @@ def run_reference(args):
 
 def run_ours(args):
     import torch
+    from scratch_wadge_b200 import replicas as RP
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
-    pg = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    pg = RP.init("nccl", 120.0)
 
     from scratch_wadge_b200 import build as B
     from scratch_wadge_b200 import capi
@@ -228,6 +222,7 @@ def run_ours(args):
         app.rk_run(dt, args.warmup + args.steps, graph=False)
         barrier()
         app.close()
+        RP.finish(pg)
         return
     # warm-up (also captures the time-step graphs) and the choice between the
     # two stage implementations: three reference kernels or the fused kernel
@@ -240,10 +235,7 @@ def run_ours(args):
     use_fused = variants["fused"] < variants["three_kernels"]
     if args.stage_variant != "auto":  # pinned (profiling: timings under a profiler mislead the choice)
         use_fused = args.stage_variant == "fused"
-    if pg:  # every rank takes the same variant
-        t = torch.tensor([1.0 if use_fused else 0.0], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        use_fused = bool(t.item() > 0)
+    use_fused = RP.agree(pg, use_fused)  # every rank takes the same variant
     app.set_fused(use_fused)
     app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     app.rk_run(dt, max(args.warmup, 1), graph=True)
@@ -258,11 +250,8 @@ def run_ours(args):
         barrier()
     ms = ev0.elapsed_time(ev1)
     clocks = clk.summary()
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ws * dofs * 5 * args.steps / (ms * 1e-3)
+    ms = RP.all_max(pg, ms)
+    value = RP.job_throughput(ws, dofs * 5 * args.steps, ms * 1e-3)
 
     # per-kernel device times (CUDA events on the app stream): the fused stage
     # kernel the time step runs, and the three reference kernels one by one
@@ -320,11 +309,8 @@ def run_ours(args):
         app.solve_host(host["Q"], host["rhsQ"], host["Qf"], dt, E2E_STEPS, resQ0=host["resQ"], out=qo)
     barrier()
     e2e_s = time.perf_counter() - t0
-    if pg:
-        t = torch.tensor([e2e_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_v = ws * dofs * 5 * E2E_STEPS * e2e_calls / e2e_s
+    e2e_s = RP.all_max(pg, e2e_s)
+    e2e_v = RP.job_throughput(ws, dofs * 5 * E2E_STEPS * e2e_calls, e2e_s)
     h2d = sum(v.nbytes for v in host.values())
     d2h = qo.nbytes
 
@@ -355,9 +341,7 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     app.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    RP.finish(pg)
 
 
 def run_adjoint_measurement(nhex=8, nsteps=200, every=20, reps=3, fd_dirs=2):
