@@ -46,8 +46,11 @@ int after_launch(const char *name) { return cuda_check(cudaGetLastError(), name)
 constexpr int pickE(int target, int per) { return per >= target ? 1 : target / per; }
 
 template <int DIM, int N> constexpr int volE() { return pickE(320, Elem<DIM, N>::NN); }
+// surface: small CTAs (2 elements at N=3) with ~64 registers per thread
+// (WADG_SURF_OCC in wadg_kernels.cuh) -- the fastest of a sweep of CTA size x
+// register cap on the 3D N=3 workload (0.072 ms vs 0.088 ms at 5 elements)
 template <int DIM, int N> constexpr int surfE() {
-  return pickE(256, Elem<DIM, N>::NfqNf > Elem<DIM, N>::Nq ? Elem<DIM, N>::NfqNf : Elem<DIM, N>::Nq);
+  return pickE(128, Elem<DIM, N>::NfqNf > Elem<DIM, N>::Nq ? Elem<DIM, N>::NfqNf : Elem<DIM, N>::Nq);
 }
 template <int DIM, int N> constexpr int updE() { return pickE(256, Elem<DIM, N>::Nq); }
 

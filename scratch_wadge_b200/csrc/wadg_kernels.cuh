@@ -272,14 +272,25 @@ update_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ V
   const int k0 = blockIdx.x * E;
   const int kend = min(K - k0, E);
 
+  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
+  const bool valid = e < kend;
+  const size_t id = (size_t)k * Nq * Nf + i;
+  // this thread's LSRK operands, loaded first so that their latency overlaps
+  // the staging of the RHS block
+  double res0[Nf], q0[Nf];
+  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
+  if (valid) {
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) {
+      res0[f] = resQ[id + f * Nq];
+      q0[f] = Q[id + f * Nq];
+    }
+  }
+
   // the E elements' rhsQ blocks are one contiguous range: copy it flat
   const double *src = rhsQ + (size_t)k0 * Nf * Nq;
   for (int t = threadIdx.x; t < kend * Nf * Nq; t += blockDim.x) (&s[0][0][0])[t] = src[t];
   __syncthreads();
-
-  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
-  const bool valid = e < kend;
-  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
 
   auto matvec = [&](const double *Op, int ld, int row, double (*X)[Nq], double *out) {
 #pragma unroll
@@ -308,14 +319,12 @@ update_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ V
 
   double V[Nf];
   if (valid) {
-    const size_t id = (size_t)k * Nq * Nf + i;
     double U[Nf];
 #pragma unroll
     for (int f = 0; f < Nf; ++f) {
-      double res = resQ[id + f * Nq];
-      res = fa * res + fdt * r[f];
+      const double res = fa * res0[f] + fdt * r[f];
       resQ[id + f * Nq] = res;
-      U[f] = Q[id + f * Nq] + fb * res;
+      U[f] = q0[f] + fb * res;
       Q[id + f * Nq] = U[f];
     }
     VU<DIM>(U, V, P);
