@@ -134,39 +134,54 @@ int launch_pairs(const wadg_adjoint *j, cudaStream_t s, const double *uq, const 
   return ck(cudaGetLastError(), "adjoint pair kernel");
 }
 
+// projection adjoint of a stage; with seed_next, also the seed of the next
+// stage of the reverse sweep (coefficient bn, step dtn)
 template <int DIM, int N, bool CURVED>
-int launch_proj(const wadg_adjoint *j, cudaStream_t s, const double *Qs, double ra, double rb) {
+int launch_proj(const wadg_adjoint *j, cudaStream_t s, const double *Qs, double ra, double rb,
+                bool seed_next, double bn, double dtn) {
   const wadg_app *a = j->app;
   constexpr int E = pickE(256, Elem<DIM, N>::Nq);
   using C = AdjProjCfg<DIM, N, E>;
-  auto kern = adj_proj_kernel<DIM, N, CURVED, E>;
-  static bool attr = false;
-  if (int r = set_smem(kern, C::smem, attr, "adjoint projection kernel smem attribute")) return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VfPqT, Qs,
-                                                              j->vbar, j->vfbar, ra, rb, j->Qbar,
-                                                              j->resbar, j->phys);
+  static_assert(C::smem >= sizeof(double) * 2 * E * Elem<DIM, N>::Nfields * Elem<DIM, N>::Nq,
+                "the seed reuses the projection's shared memory");
+  auto kern = seed_next ? adj_proj_kernel<DIM, N, CURVED, E, true> : adj_proj_kernel<DIM, N, CURVED, E, false>;
+  static bool attr[2] = {false, false};
+  if (int r = set_smem(kern, C::smem, attr[seed_next], "adjoint projection kernel smem attribute"))
+    return r;
+  kern<<<(a->K + E - 1) / E, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VfPqT, Qs, j->vbar,
+                                                      j->vfbar, ra, rb, j->Qbar, j->resbar, j->phys,
+                                                      j->VqLqT, bn, dtn, j->rhsbar, j->sfbar);
   return ck(cudaGetLastError(), "adjoint projection kernel");
 }
 
+// the three launches of a stage adjoint: seed (unless the previous stage's
+// projection kernel already seeded this one), pairs, projection (seeding the
+// next stage when there is one)
+struct StageStep {
+  const double *Qs, *uq, *uf;
+  double ra, rb, dt;
+  bool seeded;           // rhsbar / sfbar already hold this stage's seed
+  bool has_next;         // seed the next stage of the reverse sweep
+  double bn, dtn;        // its coefficient and step
+};
+
 template <int DIM, int N, bool CURVED>
-int stage_adjoint_t(const wadg_adjoint *j, cudaStream_t s, const double *Qs, const double *uq,
-                    const double *uf, double ra, double rb, double dt) {
-  int r = launch_seed<DIM, N, CURVED>(j, s, rb, dt);
-  if (!r) r = launch_pairs<DIM, N, CURVED>(j, s, uq, uf);
-  if (!r) r = launch_proj<DIM, N, CURVED>(j, s, Qs, ra, rb);
+int stage_adjoint_t(const wadg_adjoint *j, cudaStream_t s, const StageStep &st) {
+  int r = st.seeded ? WADG_OK : launch_seed<DIM, N, CURVED>(j, s, st.rb, st.dt);
+  if (!r) r = launch_pairs<DIM, N, CURVED>(j, s, st.uq, st.uf);
+  if (!r) r = launch_proj<DIM, N, CURVED>(j, s, st.Qs, st.ra, st.rb, st.has_next, st.bn, st.dtn);
   return r;
 }
 
-// adjoint of one stage with coefficients (ra, rb, dt) at the taped state
-// (Qs, uq, uf), on stream s: updates Qbar and resbar in place
-int stage_adjoint(const wadg_adjoint *j, cudaStream_t s, const double *Qs, const double *uq,
-                  const double *uf, double ra, double rb, double dt) {
+// adjoint of one stage at the taped state, on stream s: updates Qbar and
+// resbar in place
+int stage_adjoint(const wadg_adjoint *j, cudaStream_t s, const StageStep &st) {
   const wadg_app *a = j->app;
   const int dim = a->p.dim, N = a->p.N;
-#define WADG_ADJ_CASE(D_, N_)                                                           \
-  if (dim == D_ && N == N_)                                                             \
-    return a->curved ? stage_adjoint_t<D_, N_, true>(j, s, Qs, uq, uf, ra, rb, dt)      \
-                     : stage_adjoint_t<D_, N_, false>(j, s, Qs, uq, uf, ra, rb, dt);
+#define WADG_ADJ_CASE(D_, N_)                                                  \
+  if (dim == D_ && N == N_)                                                    \
+    return a->curved ? stage_adjoint_t<D_, N_, true>(j, s, st)                 \
+                     : stage_adjoint_t<D_, N_, false>(j, s, st);
   WADG_ADJ_CASE(2, 1) WADG_ADJ_CASE(2, 2) WADG_ADJ_CASE(2, 3) WADG_ADJ_CASE(2, 4)
   WADG_ADJ_CASE(3, 1) WADG_ADJ_CASE(3, 2) WADG_ADJ_CASE(3, 3) WADG_ADJ_CASE(3, 4)
 #undef WADG_ADJ_CASE
@@ -402,9 +417,13 @@ int wadg_adjoint_reverse(wadg_adjoint *j, const double *QbarT, double *Qbar0) {
     if ((r = ck(cudaStreamWaitEvent(sv, j->evR[b], 0), "event"))) return r;
     for (int idx = n * 5 - 1; idx >= 0; --idx) {
       const int st = idx % 5;
-      if ((r = stage_adjoint(j, sv, j->tapeQ[b] + idx * j->nv, j->tapeU[b] + idx * j->nv,
-                             j->tapeUf[b] + idx * j->nf, RK4A[st], RK4B[st], dt)))
-        return r;
+      // the stage before this one in the run (the next of the reverse sweep)
+      // has coefficient RK4B[(st + 4) % 5]; the sweep's last stage seeds none
+      const bool first = seg == last && idx == n * 5 - 1, final = seg == 0 && idx == 0;
+      const StageStep step{j->tapeQ[b] + idx * j->nv, j->tapeU[b] + idx * j->nv,
+                           j->tapeUf[b] + idx * j->nf, RK4A[st], RK4B[st], dt,
+                           !first, !final, RK4B[(st + 4) % 5], dt};
+      if ((r = stage_adjoint(j, sv, step))) return r;
     }
     if ((r = ck(cudaEventRecord(j->evV[b], sv), "event"))) return r;
     if (seg > 0) {
@@ -449,7 +468,8 @@ int wadg_adjoint_rhs_vjp(wadg_adjoint *j, const double *Q, const double *w, doub
   // (0, w) leaves Qbar = (dR/dQ)^T w
   if ((r = ck(cudaMemsetAsync(j->Qbar, 0, j->nv * sizeof(double), s), "memset"))) return r;
   if ((r = d2d(j->resbar, w, j->nv, s))) return r;
-  if ((r = stage_adjoint(j, s, j->sQ, j->suq, j->suf, 0.0, 0.0, 1.0))) return r;
+  const StageStep step{j->sQ, j->suq, j->suf, 0.0, 0.0, 1.0, false, false, 0.0, 0.0};
+  if ((r = stage_adjoint(j, s, step))) return r;
   return d2d(Qbar, j->Qbar, j->nv, s);
 }
 

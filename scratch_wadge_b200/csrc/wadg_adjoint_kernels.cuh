@@ -261,23 +261,22 @@ template <int DIM, int N, int E> struct AdjSeedCfg {
   static constexpr size_t smem = sizeof(double) * 2 * E * El::Nfields * El::Nq;
 };
 
+// Seed of a stage adjoint from w (this thread's node, all fields) for the
+// E elements of the block: rhsbar = Minv^T w and sfbar = VqLq^T rhsbar.
+// Called by every thread of the block (it synchronises); sA and sB are two
+// [E][Nf][Nq] shared-memory blocks.
 template <int DIM, int N, bool CURVED, int E>
-__global__ void __launch_bounds__(AdjSeedCfg<DIM, N, E>::threads)
-adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
-                const double *__restrict__ VqLqT, double b, double dt,
-                const double *__restrict__ Qbar, const double *__restrict__ resbar,
-                double *__restrict__ rhsbar, double *__restrict__ sfbar) {
+__device__ __forceinline__ void seed_block(int k0, int kend, int e, int i, bool valid,
+                                           const double *w, double Jqi,
+                                           const double *__restrict__ VqPqT,
+                                           const double *__restrict__ VqLqT, double *smem,
+                                           double *__restrict__ rhsbar,
+                                           double *__restrict__ sfbar) {
   using El = Elem<DIM, N>;
   constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
-  extern __shared__ double smem[];
   double (*sA)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
   double (*sB)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
-  const int k0 = blockIdx.x * E;
-  const int kend = min(K - k0, E);
-  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
-  const bool valid = e < kend;
-  const size_t id = (size_t)k * Nq * Nf + i;
-  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
+  const size_t id = (size_t)(k0 + e) * Nq * Nf + i;
 
   // transposed matvec from the stored transpose: out[f] = sum_j OpT(row, j) X[f][j]
   // (OpT column-major with ld rows; consecutive threads read consecutive rows)
@@ -285,18 +284,15 @@ adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
 #pragma unroll
     for (int f = 0; f < Nf; ++f) out[f] = 0.0;
     for (int j = 0; j < Nq; ++j) {
-      const double w = __ldg(OpT + row + j * ld);
+      const double wt = __ldg(OpT + row + j * ld);
 #pragma unroll
-      for (int f = 0; f < Nf; ++f) out[f] = fma(w, X[f][j], out[f]);
+      for (int f = 0; f < Nf; ++f) out[f] = fma(wt, X[f][j], out[f]);
     }
   };
 
   if (valid) {
 #pragma unroll
-    for (int f = 0; f < Nf; ++f) {
-      const double w = dt * fma(b, Qbar[id + f * Nq], resbar[id + f * Nq]);
-      sA[e][f][i] = CURVED ? w : -2.0 * w / Jqi;
-    }
+    for (int f = 0; f < Nf; ++f) sA[e][f][i] = CURVED ? w[f] : -2.0 * w[f] / Jqi;
   }
   __syncthreads();
   double r[Nf];
@@ -323,12 +319,36 @@ adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
   // sfbar(f) = sum_i VqLq(i, f) rhsbar(i)
   for (int t = threadIdx.x; t < kend * NF; t += blockDim.x) {
     const int ee = t / NF, fn = t % NF;
-    double s[Nf];
-    matvecT(VqLqT, NF, fn, sB[ee], s);
+    double sv[Nf];
+    matvecT(VqLqT, NF, fn, sB[ee], sv);
     double *out = sfbar + (size_t)(k0 + ee) * NF * Nf + fn;
 #pragma unroll
-    for (int f = 0; f < Nf; ++f) out[f * NF] = s[f];
+    for (int f = 0; f < Nf; ++f) out[f * NF] = sv[f];
   }
+}
+
+template <int DIM, int N, bool CURVED, int E>
+__global__ void __launch_bounds__(AdjSeedCfg<DIM, N, E>::threads)
+adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
+                const double *__restrict__ VqLqT, double b, double dt,
+                const double *__restrict__ Qbar, const double *__restrict__ resbar,
+                double *__restrict__ rhsbar, double *__restrict__ sfbar) {
+  using El = Elem<DIM, N>;
+  constexpr int Nq = El::Nq, Nf = El::Nfields;
+  extern __shared__ double smem[];
+  const int k0 = blockIdx.x * E;
+  const int kend = min(K - k0, E);
+  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
+  const bool valid = e < kend;
+  const size_t id = (size_t)k * Nq * Nf + i;
+  double w[Nf];
+  double Jqi = 1.0;
+  if (valid) {
+    Jqi = Jq[(size_t)k * Nq + i];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) w[f] = dt * fma(b, Qbar[id + f * Nq], resbar[id + f * Nq]);
+  }
+  seed_block<DIM, N, CURVED, E>(k0, kend, e, i, valid, w, Jqi, VqPqT, VqLqT, smem, rhsbar, sfbar);
 }
 
 // ------------------------------------------------------------------ pairs
@@ -732,12 +752,17 @@ template <int DIM, int N, int E> struct AdjProjCfg {
   static constexpr size_t smem = sizeof(double) * E * El::Nfields * (2 * El::Nq + El::NfqNf);
 };
 
-template <int DIM, int N, bool CURVED, int E>
+// SEED = true: then seeds the next stage of the reverse sweep (coefficient bn,
+// step dtn) from the updated adjoints, as adj_seed_kernel would (its rhsbar
+// and sfbar are free: this stage's pair kernel has finished with them).
+template <int DIM, int N, bool CURVED, int E, bool SEED>
 __global__ void __launch_bounds__(AdjProjCfg<DIM, N, E>::threads)
 adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
                 const double *__restrict__ VfPqT, const double *__restrict__ Qs,
                 const double *__restrict__ vbar, const double *__restrict__ vfbar, double a,
-                double b, double *__restrict__ Qbar, double *__restrict__ resbar, Phys P) {
+                double b, double *__restrict__ Qbar, double *__restrict__ resbar, Phys P,
+                const double *__restrict__ VqLqT, double bn, double dtn,
+                double *__restrict__ rhsbar, double *__restrict__ sfbar) {
   using El = Elem<DIM, N>;
   constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
   extern __shared__ double smem[];
@@ -803,18 +828,27 @@ adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__
       for (int f = 0; f < Nf; ++f) x[f] *= Jqi;
     }
   }
-  if (!valid) return;
   const size_t id = (size_t)k * Nq * Nf + i;
-  double U[Nf], Ub[Nf];
+  double wn[Nf];
+  if (valid) {
+    double U[Nf], Ub[Nf];
 #pragma unroll
-  for (int f = 0; f < Nf; ++f) U[f] = Qs[id + f * Nq];
-  adj::VU_vjp<DIM>(U, x, gas_of(P), Ub);
+    for (int f = 0; f < Nf; ++f) U[f] = Qs[id + f * Nq];
+    adj::VU_vjp<DIM>(U, x, gas_of(P), Ub);
 #pragma unroll
-  for (int f = 0; f < Nf; ++f) {
-    const double qb = Qbar[id + f * Nq];
-    const double rt = fma(b, qb, resbar[id + f * Nq]);
-    resbar[id + f * Nq] = a * rt;
-    Qbar[id + f * Nq] = qb + Ub[f];
+    for (int f = 0; f < Nf; ++f) {
+      const double qb = Qbar[id + f * Nq];
+      const double rt = fma(b, qb, resbar[id + f * Nq]);
+      const double rn = a * rt, qn = qb + Ub[f];
+      resbar[id + f * Nq] = rn;
+      Qbar[id + f * Nq] = qn;
+      wn[f] = dtn * fma(bn, qn, rn);
+    }
+  }
+  if (SEED) {
+    __syncthreads();  // every thread is done with sV / sX
+    seed_block<DIM, N, CURVED, E>(k0, kend, e, i, valid, wn, Jqi, VqPqT, VqLqT, smem, rhsbar,
+                                  sfbar);
   }
 }
 
