@@ -249,7 +249,8 @@ class App:
         return ms.value
 
     def set_fused(self, fused: bool):
-        """fused stage kernel (default) or the three reference kernels per stage"""
+        """fused stage kernel (one launch per stage) or, the default, the three
+        reference kernels per stage"""
         check(lib().wadg_app_set_fused(self.h, int(fused)), "set_fused")
 
     def time_stage(self, dt, nstages):

@@ -17,11 +17,14 @@
 //                     penalty), then the adjoints of the primitive recovery
 //                     and of U(V~) at each volume and face node: vbar, vfbar
 //   adj_proj_kernel   the adjoint of the entropy projection and of V(Q), and
-//                     the LSRK adjoint update of Qbar and resbar.
+//                     the LSRK adjoint update of Qbar and resbar; in a reverse
+//                     sweep it also seeds the next stage (so adj_seed_kernel
+//                     runs only for the sweep's first stage).
 // Neighbour contributions of the surface term are gathered, not scattered:
 // face node j adds the P-side derivative of the evaluation made at its
-// neighbour m = mapPq(j), which needs sfbar at m (hence the separate seed
-// kernel) and mapPq(m) = j (a conforming face pairing; checked on the host).
+// neighbour m = mapPq(j), which needs sfbar at m -- computed, for every
+// element, before the pair kernel starts -- and mapPq(m) = j (a conforming
+// face pairing; checked on the host).
 #pragma once
 
 #include "wadg_adjoint_math.cuh"
