@@ -59,6 +59,15 @@ typedef struct
 int wadg_ctx_create(const wadg_params *p, wadg_ctx **out);
 int wadg_ctx_destroy(wadg_ctx *ctx);
 int wadg_ctx_set_stream(wadg_ctx *ctx, void *stream);
+/* Tiling of the pair volume kernel: warps per CTA (elements per CTA follow
+ * from it; results do not depend on it).  wadg_vol_warps_candidates writes
+ * the compiled shapes for the context's degree (at most 3; the first is the
+ * default) and returns their number; wadg_ctx_set_vol_warps selects one
+ * (0 = the default).  No counterpart in the reference (OCCA's inner-loop
+ * sizes are fixed defines); wadg_app_autotune picks one by timing. */
+int wadg_vol_warps_candidates(const wadg_ctx *ctx, int curved, int *out);
+int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps);
+int wadg_ctx_get_vol_warps(const wadg_ctx *ctx);
 const char *wadg_last_error(void);
 /* degrees compiled for `dim`, as a bit mask (bit N set = degree N) */
 int wadg_supported_degrees(int dim);
@@ -225,8 +234,20 @@ int wadg_app_time_kernels(wadg_app *app, double dt, int nstages, float *ms);
  * ms receives the total. */
 int wadg_app_time_stage(wadg_app *app, double dt, int nstages, float *ms);
 
+/* Autotuner: times `nstages` LSRK stages (three kernels, CUDA events) with
+ * each compiled CTA shape of the volume kernel on the app's own mesh and
+ * state, keeps the fastest (written to *warps; times, if not NULL, receives
+ * the volume kernel's ms per launch for each candidate in the order of
+ * wadg_vol_warps_candidates) and leaves it selected for the app's kernels.
+ * Advances the app's state: call it before set_state. */
+int wadg_app_autotune(wadg_app *app, double dt, int nstages, int *warps,
+                      float *times);
+
 /* the app's CUDA stream (a cudaStream_t) */
 void *wadg_app_stream(wadg_app *app);
+/* the app's kernel context (for wadg_ctx_* settings such as the volume
+ * kernel's CTA shape) */
+wadg_ctx *wadg_app_ctx(wadg_app *app);
 /* fused-stage ping-pong: which state buffer is current (0 or 1).  The state
  * accessors read the current buffer; set only to undo a capture. */
 int wadg_app_set_parity(wadg_app *app, int parity);

@@ -79,6 +79,8 @@ def lib():
         L.wadg_app_time_stage.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
         L.wadg_probe_fp64_fma.argtypes = [v, i, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_float)]
+        L.wadg_app_ctx.restype = ctypes.c_void_p
+        L.wadg_app_ctx.argtypes = [v]
         L.wadg_app_stream.restype = ctypes.c_void_p
         L.wadg_app_stream.argtypes = [v]
         L.wadg_app_set_parity.argtypes = [v, i]
@@ -92,6 +94,11 @@ def lib():
         L.wadg_app_destroy.argtypes = [v]
         L.wadg_app_sync.argtypes = [v]
         L.wadg_ctx_set_stream.argtypes = [v, v]
+        L.wadg_vol_warps_candidates.argtypes = [v, i, ctypes.POINTER(ctypes.c_int)]
+        L.wadg_ctx_set_vol_warps.argtypes = [v, i, i]
+        L.wadg_ctx_get_vol_warps.argtypes = [v]
+        L.wadg_app_autotune.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_float)]
         L.wadg_adjoint_create.argtypes = [v, i, i, ctypes.POINTER(ctypes.c_void_p)]
         L.wadg_adjoint_destroy.argtypes = [v]
         L.wadg_adjoint_forward.argtypes = [v, v, d, v]
@@ -262,6 +269,18 @@ class App:
         ms = (ctypes.c_float * 3)()
         check(lib().wadg_app_time_kernels(self.h, dt, nstages, ms), "time_kernels")
         return list(ms)
+
+    def autotune(self, dt, nstages=10):
+        """Pick the volume kernel's CTA shape by timing each compiled one on
+        this app (advances the state: set it afterwards).  Returns
+        (chosen warps per CTA, {warps: ms per volume launch})."""
+        w = ctypes.c_int()
+        t = (ctypes.c_float * 3)()
+        check(lib().wadg_app_autotune(self.h, dt, nstages, ctypes.byref(w), t), "autotune")
+        ctx = ctypes.c_void_p(lib().wadg_app_ctx(self.h))
+        cand = (ctypes.c_int * 3)()
+        n = lib().wadg_vol_warps_candidates(ctx, int(self.curved), cand)
+        return w.value, {int(cand[k]): float(t[k]) for k in range(n)}
 
 
 class Solver:

@@ -430,6 +430,35 @@ int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
   return WADG_OK;
 }
 
+int wadg_app_autotune(wadg_app *a, double dt, int nstages, int *warps, float *times) {
+  if (!a || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  int cand[3];
+  const int n = wadg_vol_warps_candidates(a->ctx, a->curved, cand);
+  if (n <= 0) return afail(WADG_ERR_UNSUPPORTED, "no volume kernel shapes");
+  int best = cand[0];
+  float best_ms = -1.0f;
+  for (int i = 0; i < n; ++i) {
+    int r = wadg_ctx_set_vol_warps(a->ctx, a->curved, cand[i]);
+    float ms[3] = {0, 0, 0};
+    if (!r) r = wadg_app_time_kernels(a, dt, 1, ms);  // warm-up: attributes, caches
+    if (!r) r = wadg_app_time_kernels(a, dt, nstages, ms);
+    if (r) return r;
+    if (times) times[i] = ms[0] / nstages;
+    if (best_ms < 0.0f || ms[0] < best_ms) {
+      best_ms = ms[0];
+      best = cand[i];
+    }
+  }
+  // graphs captured with another shape are stale
+  for (auto &g : a->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  if (warps) *warps = best;
+  return wadg_ctx_set_vol_warps(a->ctx, a->curved, best);
+}
+
 int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {
   if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
   const int fused = a->fused;
@@ -452,6 +481,7 @@ int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {
 }
 
 void *wadg_app_stream(wadg_app *a) { return a ? (void *)a->stream : nullptr; }
+wadg_ctx *wadg_app_ctx(wadg_app *a) { return a ? a->ctx : nullptr; }
 
 int wadg_app_set_parity(wadg_app *a, int parity) {
   if (!a || (parity != 0 && parity != 1)) return afail(WADG_ERR_INVALID, "invalid argument");

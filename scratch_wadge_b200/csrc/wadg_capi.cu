@@ -20,6 +20,7 @@ struct wadg_ctx {
   int dim, N, Nq, Nfq, Nfaces;
   Phys phys;
   cudaStream_t stream;
+  int vol_warps = 0;  // warps per CTA of the pair volume kernel; 0 = the default
 };
 
 namespace {
@@ -94,12 +95,20 @@ int num_sms() {
   return n;
 }
 
+// candidate CTA shapes of the pair volume kernel (warps per CTA; elements per
+// CTA = warps / 2 * 32 / lanes per element): the largest that fits in shared
+// memory, and two and four warps fewer
 template <int DIM, int N, bool CURVED>
-int launch_vol_pairs(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
-                     const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
-                     const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
-                     const double *Qf, double *rhsQ, double *rhsQf) {
-  constexpr int W = volpairsW<DIM, N, CURVED>();
+constexpr int volpairsW_cand(int i) {
+  constexpr int W0 = volpairsW<DIM, N, CURVED>();
+  return i == 0 ? W0 : (W0 - 2 * i >= 2 ? W0 - 2 * i : 0);
+}
+
+template <int DIM, int N, bool CURVED, int W>
+int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                       const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+                       const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
+                       const double *Qf, double *rhsQ, double *rhsQf) {
   using C = VolPairsCfg<DIM, N, CURVED, W>;
   static_assert(C::smem <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
   auto kern = vol_pairs_kernel<DIM, N, CURVED, W>;
@@ -115,6 +124,31 @@ int launch_vol_pairs(const wadg_ctx *c, int K, const double *vgeo, const double 
   kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
                                                   VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
   return after_launch("volume kernel");
+}
+
+// the context's CTA shape (wadg_ctx_set_vol_warps), else the default
+template <int DIM, int N, bool CURVED>
+int launch_vol_pairs(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                     const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
+                     const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
+                     const double *Qf, double *rhsQ, double *rhsQf) {
+  constexpr int W1 = volpairsW_cand<DIM, N, CURVED>(1), W2 = volpairsW_cand<DIM, N, CURVED>(2);
+  if (W1 && c->vol_warps == W1)
+    return launch_vol_pairs_w<DIM, N, CURVED, (W1 ? W1 : 2)>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq,
+                                                             Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf);
+  if (W2 && c->vol_warps == W2)
+    return launch_vol_pairs_w<DIM, N, CURVED, (W2 ? W2 : 2)>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq,
+                                                             Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf);
+  return launch_vol_pairs_w<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>(
+      c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf);
+}
+
+template <int DIM, int N, bool CURVED>
+int vol_warps_candidates(int *out) {
+  int n = 0;
+  for (int i = 0; i < 3; ++i)
+    if (int w = volpairsW_cand<DIM, N, CURVED>(i)) out[n++] = w;
+  return n;
 }
 
 template <int DIM, int N, bool CURVED>
@@ -300,6 +334,31 @@ int wadg_ctx_set_stream(wadg_ctx *ctx, void *stream) {
   ctx->stream = (cudaStream_t)stream;
   return WADG_OK;
 }
+
+int wadg_vol_warps_candidates(const wadg_ctx *ctx, int curved, int *out) {
+  if (!ctx || !out) return -fail(WADG_ERR_INVALID, "null argument");
+  const wadg_ctx *c = ctx;
+  if (curved) {
+    WADG_DISPATCH(c, return (vol_warps_candidates<D_, N_, true>(out)));
+  } else {
+    WADG_DISPATCH(c, return (vol_warps_candidates<D_, N_, false>(out)));
+  }
+}
+
+int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps) {
+  if (!ctx) return fail(WADG_ERR_INVALID, "null context");
+  if (warps != 0) {
+    int cand[3];
+    const int n = wadg_vol_warps_candidates(ctx, curved, cand);
+    bool ok = false;
+    for (int i = 0; i < n; ++i) ok = ok || cand[i] == warps;
+    if (!ok) return fail(WADG_ERR_INVALID, "%d warps per CTA is not a compiled shape", warps);
+  }
+  ctx->vol_warps = warps;
+  return WADG_OK;
+}
+
+int wadg_ctx_get_vol_warps(const wadg_ctx *ctx) { return ctx ? ctx->vol_warps : -1; }
 
 // ------------------------------------------------------------------ 3D
 int wadg_euler_vol_3d(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,

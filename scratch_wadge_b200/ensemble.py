@@ -92,7 +92,7 @@ def common_dt(parts, CFL=0.5):
 class Ensemble:
     """The batched path."""
 
-    def __init__(self, instances, parts=None, fused=False, gamma=1.4):
+    def __init__(self, instances, parts=None, fused=False, gamma=1.4, autotune_dt=None):
         self.instances = instances
         self.parts = parts if parts is not None else [build_instance(i, gamma) for i in instances]
         self.degrees = sorted({i.N for i in instances})
@@ -102,8 +102,12 @@ class Ensemble:
             geo, st, offs = concat([self.parts[j] for j in idx])
             app = capi.App(geo, curved=True, gamma=gamma)
             app.set_fused(fused)
+            tuning = None
+            if autotune_dt is not None:  # the volume kernel's CTA shape for this bin
+                app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
+                tuning = app.autotune(autotune_dt)
             app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
-            self.bins[N] = dict(idx=idx, geo=geo, state=st, offs=offs, app=app)
+            self.bins[N] = dict(idx=idx, geo=geo, state=st, offs=offs, app=app, tuning=tuning)
         apps = (ctypes.c_void_p * len(self.bins))(*[b["app"].h.value for b in self.bins.values()])
         h = ctypes.c_void_p()
         L = capi.lib()
