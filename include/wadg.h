@@ -145,6 +145,19 @@ int wadg_euler_update_2d_curved(wadg_ctx *ctx, int K, const double *Jq,
                                 double fa, double fb, double fdt, double *rhsQ,
                                 double *resQ, double *Q, double *Qf);
 
+/* ------------------------------------------------------------ diagnostics
+ * euler_3d_compute_aux: Euler3D.okl:3888 -- aux[k] = sum_i 1/2 |m|^2/rho J w,
+ * the kinetic energy of element k (the reference sums aux on the host; its
+ * rk_run has the call compiled out, euler.c:3701-3710).  Also accepts a 2D
+ * context (two momentum components).  wq: the volume cubature weights [Nq].
+ * wadg_element_entropy: S[k] = sum_i w J (-rho s), s = log((gamma-1) rhoe /
+ * rho^gamma) -- the per-element terms of the entropy the reference's driver
+ * sums on the host (euler.c:4135-4156, 4276-4315). */
+int wadg_euler_3d_compute_aux(wadg_ctx *ctx, int K, const double *Jq,
+                              const double *wq, const double *Q, double *aux);
+int wadg_element_entropy(wadg_ctx *ctx, int K, const double *Jq,
+                         const double *wq, const double *Q, double *S);
+
 /* ------------------------------------------------------------ fused stage
  * One LSRK stage -- vol, surf and update of the kernels above -- in a single
  * launch (rk_step, euler.c:3610-3666, with rhsQf and the volume RHS kept on

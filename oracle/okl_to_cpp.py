@@ -33,7 +33,8 @@ reference fails loudly instead of being patched blindly:
 The rest of both files keeps its shipped TESTING configuration (its loop code
 is the variant that compiles).
 
-Only the kernels on the hot path are kept (``KERNELS``): everything before the
+Only the kernels on the hot path (and Euler3D.okl's per-element kinetic-energy
+diagnostic, euler_3d_compute_aux) are kept (``KERNELS``): everything before the
 first ``kernel`` (macros, logmean, VU/UV, the flux functions) plus each listed
 kernel from its ``kernel void`` line up to the next one.  Other kernels of
 Euler3D.okl are experiments that do not all compile (e.g. its own
@@ -53,7 +54,8 @@ PATCHES = {
 
 KERNELS = {
     "Euler3Daffine.okl": ("euler_vol_3d", "euler_surf_3d", "euler_update_3d"),
-    "Euler3D.okl": ("euler_vol_3d_curved", "euler_surf_3d", "euler_update_3d_curved"),
+    "Euler3D.okl": ("euler_vol_3d_curved", "euler_surf_3d", "euler_update_3d_curved",
+                    "euler_3d_compute_aux"),
     "Euler2D.okl": ("euler_vol_2d", "euler_vol_2d_curved", "euler_surf_2d",
                     "euler_update_2d", "euler_update_2d_curved"),
 }

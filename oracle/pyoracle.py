@@ -188,3 +188,14 @@ class Reference(_Base):
         K = Q.shape[0]
         self._upd(K, _p(geo.Jq), _p(self.VqPq), _p(self.VfPq), fa, fb, fdt,
                   _p(rhsQ), _p(resQ), _p(Q), _p(Qf))
+
+    def compute_aux(self, geo, Q):
+        """euler_3d_compute_aux (Euler3D.okl:3888): per-element kinetic
+        energy; only the Euler3D library (3D, curved) has it."""
+        if not hasattr(self.L, "euler_3d_compute_aux"):
+            raise AttributeError("euler_3d_compute_aux is in the Euler3D (curved 3D) library")
+        K = Q.shape[0]
+        aux = np.zeros(K)
+        wq = np.ascontiguousarray(self.ops.wq, dtype=np.float64)
+        self.L.euler_3d_compute_aux(K, _p(geo.Jq), _p(wq), _p(np.ascontiguousarray(Q)), _p(aux))
+        return aux

@@ -94,6 +94,8 @@ def lib():
         L.wadg_app_destroy.argtypes = [v]
         L.wadg_app_sync.argtypes = [v]
         L.wadg_ctx_set_stream.argtypes = [v, v]
+        L.wadg_euler_3d_compute_aux.argtypes = [v, i, v, v, v, v]
+        L.wadg_element_entropy.argtypes = [v, i, v, v, v, v]
         L.wadg_vol_warps_candidates.argtypes = [v, i, ctypes.POINTER(ctypes.c_int)]
         L.wadg_ctx_set_vol_warps.argtypes = [v, i, i]
         L.wadg_ctx_get_vol_warps.argtypes = [v]
@@ -167,6 +169,14 @@ class Context:
             check(L.wadg_euler_stage_2d(self.h, K, int(curved), vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
                                         Drq, Dsq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, rhsQ_in, Qf_in,
                                         Q, resQ, rhsQ_out, Qf_out), "stage")
+
+    def compute_aux(self, K, Jq, wq, Q, aux):
+        """per-element kinetic energy (euler_3d_compute_aux)"""
+        check(lib().wadg_euler_3d_compute_aux(self.h, K, Jq, wq, Q, aux), "compute_aux")
+
+    def element_entropy(self, K, Jq, wq, Q, S):
+        """per-element entropy integral sum_i w J (-rho s)"""
+        check(lib().wadg_element_entropy(self.h, K, Jq, wq, Q, S), "element_entropy")
 
     def update(self, curved, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf):
         L = lib()

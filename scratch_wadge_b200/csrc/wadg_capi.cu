@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/wadg.h"
+#include "wadg_diag.cuh"
 #include "wadg_kernels.cuh"
 #include "wadg_vol.cuh"
 
@@ -275,6 +276,16 @@ int wadg_ctx_sizes(const wadg_ctx *c, int *dim, int *NfqNf) {
   return WADG_OK;
 }
 
+// per-element integrals (wadg_euler_3d_compute_aux, wadg_element_entropy)
+template <int DIM, int N, bool ENTROPY>
+int launch_integral(const wadg_ctx *c, int K, const double *Jq, const double *wq, const double *Q,
+                    double *out) {
+  const size_t threads = (size_t)K * 32;
+  element_integral_kernel<DIM, N, ENTROPY><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+      K, Jq, wq, Q, out, c->phys);
+  return after_launch("element integral kernel");
+}
+
 extern "C" {
 
 const char *wadg_last_error(void) { return g_err.c_str(); }
@@ -359,6 +370,26 @@ int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps) {
 }
 
 int wadg_ctx_get_vol_warps(const wadg_ctx *ctx) { return ctx ? ctx->vol_warps : -1; }
+
+// ------------------------------------------------------------------ diagnostics
+
+int wadg_euler_3d_compute_aux(wadg_ctx *c, int K, const double *Jq, const double *wq,
+                              const double *Q, double *aux) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  if (K < 0) return fail(WADG_ERR_INVALID, "K < 0");
+  if (K == 0) return WADG_OK;
+  if (any_null({Jq, wq, Q, aux})) return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_integral<D_, N_, false>(c, K, Jq, wq, Q, aux)));
+}
+
+int wadg_element_entropy(wadg_ctx *c, int K, const double *Jq, const double *wq, const double *Q,
+                         double *S) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  if (K < 0) return fail(WADG_ERR_INVALID, "K < 0");
+  if (K == 0) return WADG_OK;
+  if (any_null({Jq, wq, Q, S})) return fail(WADG_ERR_INVALID, "null pointer argument");
+  WADG_DISPATCH(c, return (launch_integral<D_, N_, true>(c, K, Jq, wq, Q, S)));
+}
 
 // ------------------------------------------------------------------ 3D
 int wadg_euler_vol_3d(wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
