@@ -11,13 +11,15 @@
 // Layout.  A group of L lanes owns one element; lane l owns the R volume rows
 // i = l + L*r (register accumulators; the padding row, if any, computes on a
 // clamped index and is never stored).  Two warps share each group of G = 32/L
-// elements: warp h walks half of the volume columns j and half of the face
-// steps s.  At face step s lane l takes face node f = (l + s) mod NfqNf, so the
-// L lanes of a group always touch L distinct face rows; each adds its R
-// contributions to its warp's copy of the face-row accumulators in shared
-// memory, and a __syncwarp between steps orders the read-modify-writes.  The
-// schedule is fixed, so results are deterministic (no atomics).  Warps stay
-// converged throughout so that ecflux_n_warp can vote on the log-mean branch.
+// elements (one where a half of the face nodes would be fewer than L): warp h
+// walks half of the volume columns j and its own half of the face nodes,
+// [f0_h, f0_h + n_h).  At face step s lane l takes face node
+// f = f0_h + (l + s) mod n_h, so the L lanes of a group always touch L distinct
+// face rows, and the two warps never the same one: both add their R
+// contributions to one copy of the face-row accumulators in shared memory, a
+// __syncwarp between steps ordering the read-modify-writes.  The schedule is
+// fixed, so results are deterministic (no atomics).  Warps stay converged
+// throughout so that ecflux_n_warp can vote on the log-mean branch.
 //
 // Persistent CTAs: operator tables are staged in shared memory once per CTA;
 // the face weights in a rotated layout [r][s][l] so that the lanes of a step
@@ -35,19 +37,23 @@ template <int DIM, int N> struct VolTile {
   static constexpr int R = (El::Nq + L - 1) / L;
   static constexpr int G = 32 / L;  // elements per warp group
   static_assert(El::NfqNf >= L, "face schedule needs NfqNf >= L");
+  // face halves of the two warps of an element (the second may be empty)
+  static constexpr int nf0 = (El::NfqNf + 1) / 2, nf1 = El::NfqNf - nf0;
+  static constexpr int H = nf1 >= L ? 2 : 1;  // warps per element group
+  __host__ __device__ static constexpr int nf(int h) { return H == 1 ? El::NfqNf : (h ? nf1 : nf0); }
+  __host__ __device__ static constexpr int f0(int h) { return h ? nf0 : 0; }
 };
 
 template <int DIM, int N, bool CURVED, int W>
 struct VolPairsCfg {
   using El = Elem<DIM, N>;
   using T = VolTile<DIM, N>;
-  static constexpr int H = 2;                         // warps per element group
+  static constexpr int H = T::H;                      // warps per element group
   static constexpr int threads = 32 * W;
   static constexpr int E = (W / H) * T::G;            // elements per batch
-  // element strides in doubles: the state stride is 4 mod 8 and the stride of
-  // an element's pair of face accumulators (H*SA) is 4 mod 8, so the G groups
-  // of a warp start 8 banks apart (conflict-free broadcasts, two wavefronts
-  // for a step's consecutive face rows)
+  // element strides in doubles: the state stride and the face-accumulator
+  // stride are 4 mod 8, so the G groups of a warp start 8 banks apart
+  // (conflict-free broadcasts, two wavefronts for a step's consecutive face rows)
   static constexpr int pad4of8(int x) { return ((x + 3) / 8) * 8 + 4; }   // == 4 mod 8
   static constexpr int pad2of4(int x) { return ((x + 1) / 4) * 4 + 2; }   // == 2 mod 4
   static constexpr int NGS = CURVED ? El::Nvgeo : 0;  // geometric factors per node
@@ -55,12 +61,12 @@ struct VolPairsCfg {
   // the state block of an element is reused after the pair phase for the row
   // buffer and the update's staging arrays (3 x Nfields x Nq)
   static constexpr int SE = pad4of8(mx((El::NS + NGS) * El::NN, 3 * El::Nfields * El::Nq));
-  static constexpr int SA = pad2of4(El::Nfields * El::NfqNf);
+  static constexpr int SA = pad4of8(El::Nfields * El::NfqNf);
   static constexpr int SN = El::Nfaces * DIM + El::Nvgeo;
   static constexpr int nD = DIM * El::Nq * El::Nq;
   static constexpr int nW = T::R * El::NfqNf * T::L;
   static constexpr size_t fixed = sizeof(double) * (size_t)(nD + 2 * nW + El::Nfaces * DIM);
-  static constexpr size_t per_elem = sizeof(double) * (size_t)(SE + H * SA + SN);
+  static constexpr size_t per_elem = sizeof(double) * (size_t)(SE + SA + SN);
   static constexpr size_t smem = fixed + E * per_elem;
 };
 
@@ -79,12 +85,12 @@ struct VolPairs {
 
   __device__ __forceinline__ VolPairs(double *smem) {
     sD = smem;                     // Drq | Dsq | Dtq, column-major
-    sW1 = sD + C::nD;              // [R][NF][L]  1/2 VqLq(i, f), 0 on padding rows
-    sW2 = sW1 + C::nW;             // [R][NF][L] -1/2 VfPq(f, i), 0 on padding rows
+    sW1 = sD + C::nD;              // [h][R][n_h][L]  1/2 VqLq(i, f), 0 on padding rows
+    sW2 = sW1 + C::nW;             // [h][R][n_h][L] -1/2 VfPq(f, i), 0 on padding rows
     sNr = sW2 + C::nW;             // reference normals [Nfaces][DIM]
     sSt = sNr + El::Nfaces * DIM;  // [E][SE]     node states (+ geometric factors)
-    sAcc = sSt + E * SE;           // [E][H][SA]  face-row accumulators, one per warp
-    sNrm = sAcc + E * H * SA;      // [E][SN]     per-face nJ (affine) + G
+    sAcc = sSt + E * SE;           // [E][SA]     face-row accumulators
+    sNrm = sAcc + E * SA;          // [E][SN]     per-face nJ (affine) + G
     tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     h = warp % H;
@@ -103,10 +109,17 @@ struct VolPairs {
       if (DIM == 3) sD[2 * Nq * Nq + t] = Dtq[t];
     }
     for (int t = tid; t < C::nW; t += blockDim.x) {
-      const int ll = t % L, s = (t / L) % NF, r = t / (L * NF);
+      int hh = 0, u = t;
+      if (H == 2 && u >= R * L * T::nf(0)) {
+        hh = 1;
+        u -= R * L * T::nf(0);
+      }
+      const int n_ = T::nf(hh);
+      const int ll = u % L, s = (u / L) % n_, r = u / (L * n_);
       const int i = ll + L * r;
-      int f = ll + s;
-      if (f >= NF) f -= NF;
+      int ff = ll + s;
+      if (ff >= n_) ff -= n_;
+      const int f = T::f0(hh) + ff;
       sW1[t] = i < Nq ? 0.5 * VqLq[i + f * Nq] : 0.0;
       sW2[t] = i < Nq ? -0.5 * VfPq[f + i * NF] : 0.0;
     }
@@ -140,7 +153,7 @@ struct VolPairs {
                                            : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
       }
     }
-    for (int t = tid; t < E * H * SA; t += blockDim.x) sAcc[t] = 0.0;
+    for (int t = tid; t < E * SA; t += blockDim.x) sAcc[t] = 0.0;
     if (!CURVED) {
       for (int t = tid; t < E; t += blockDim.x) {
         const int k = min(k0 + t, K - 1);
@@ -174,11 +187,11 @@ struct VolPairs {
   }
 
   // all flux pairs of element e: this warp's half of the volume columns and of
-  // the face steps; rows into acc (registers), face rows into this warp's
-  // accumulator copy
+  // the face nodes; rows into acc (registers), face rows into the element's
+  // face accumulators
   __device__ __forceinline__ void pairs(double (&acc)[R][Nf], const Phys &P) const {
     const double *st = sSt + e * SE;
-    double *acc_f = sAcc + (e * H + h) * SA;
+    double *acc_f = sAcc + e * SA;
     NodeState<DIM> A[R];
     int ir[R];
 #pragma unroll
@@ -195,7 +208,7 @@ struct VolPairs {
     }
 
     // volume-volume pairs: warp h takes columns [j0, j1)
-    const int j0 = h ? Nq / 2 : 0, j1 = h ? Nq : Nq / 2;
+    const int j0 = (H == 2 && h) ? Nq / 2 : 0, j1 = (H == 2 && !h) ? Nq / 2 : Nq;
     for (int j = j0; j < j1; ++j) {
       const NodeState<DIM> B = load(st, j);
 #pragma unroll
@@ -221,11 +234,13 @@ struct VolPairs {
       }
     }
 
-    // volume-face pairs, each evaluated once: warp h takes steps [s0, s1)
-    const int s0 = h ? NF / 2 : 0, s1 = h ? NF : NF / 2;
-    for (int s = s0; s < s1; ++s) {
-      int f = l + s;
-      if (f >= NF) f -= NF;
+    // volume-face pairs, each evaluated once: warp h takes its face nodes
+    const int nfh = T::nf(h), f0h = T::f0(h);
+    const double *w1h = sW1 + R * L * f0h, *w2h = sW2 + R * L * f0h;
+    for (int s = 0; s < nfh; ++s) {
+      int ff = l + s;
+      if (ff >= nfh) ff -= nfh;
+      const int f = f0h + ff;
       const NodeState<DIM> B = load(st, Nq + f);
       const int fc = f / Nfq;
       double nv[DIM];
@@ -252,8 +267,8 @@ struct VolPairs {
         }
         double F[Nf];
         ecflux_n_warp<DIM>(A[r], B, nv, P, F);
-        const double w1 = sW1[(r * NF + s) * L + l];
-        const double w2 = sW2[(r * NF + s) * L + l];
+        const double w1 = w1h[(r * nfh + s) * L + l];
+        const double w2 = w2h[(r * nfh + s) * L + l];
 #pragma unroll
         for (int q = 0; q < Nf; ++q) {
           acc[r][q] = fma(w1, F[q], acc[r][q]);
@@ -317,13 +332,13 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           if (i < Nq) {
             double *out = rhsQ + (size_t)k * Nq * Nf + i;
 #pragma unroll
-            for (int q = 0; q < Nf; ++q) out[q * Nq] = acc[r][q] + rowbuf[q * Nq + i];
+            for (int q = 0; q < Nf; ++q) out[q * Nq] = H == 2 ? acc[r][q] + rowbuf[q * Nq + i] : acc[r][q];
           }
         }
       }
-      const double *a0 = v.sAcc + (v.e * H + 0) * V::SA, *a1 = v.sAcc + (v.e * H + 1) * V::SA;
+      const double *a0 = v.sAcc + v.e * V::SA;
       double *outf = rhsQf + (size_t)k * NF * Nf;
-      for (int t = v.h * L + v.l; t < NF * Nf; t += H * L) outf[t] = a0[t] + a1[t];
+      for (int t = v.h * L + v.l; t < NF * Nf; t += H * L) outf[t] = a0[t];
     }
   }
 }
@@ -368,8 +383,8 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
     __syncthreads();
 
     // ---- surface: sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam) sJ (u+ - u-)
-    // (Euler3D.okl:3256-3346, Euler2D.okl:1373-1453); stored over copy 0 of
-    // the face accumulators
+    // (Euler3D.okl:3256-3346, Euler2D.okl:1373-1453); stored over the face
+    // accumulators
     for (int t = tid; t < E * NF; t += nth) {
       const int ee = t / NF, f = t % NF, k = k0 + ee;
       if (k >= K) continue;
@@ -403,25 +418,25 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
       const double lamP = sqrt(kP) + sqrt(P.gamma * pP / UP[0]);
       const double tau = (DIM == 3) ? P.tau : 1.0;
       const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
-      double *a0 = v.sAcc + (ee * H + 0) * SA;
-      const double *a1 = v.sAcc + (ee * H + 1) * SA;
+      double *a0 = v.sAcc + ee * SA;
 #pragma unroll
-      for (int q = 0; q < Nf; ++q)
-        a0[q * NF + f] = (a0[q * NF + f] + a1[q * NF + f]) + 0.5 * F[q] - Lfc * (UP[q] - UM[q]);
+      for (int q = 0; q < Nf; ++q) a0[q * NF + f] = a0[q * NF + f] + 0.5 * F[q] - Lfc * (UP[q] - UM[q]);
     }
     __syncthreads();
 
     // ---- lift: rows += VqLq sfS, on the rotated weights (VqLq = 2 W1),
     // the two warps splitting the face nodes as in the pair phase
     {
-      const double *sf = v.sAcc + (v.e * H + 0) * SA;
-      const int s0 = v.h ? NF / 2 : 0, s1 = v.h ? NF : NF / 2;
-      for (int s = s0; s < s1; ++s) {
-        int f = v.l + s;
-        if (f >= NF) f -= NF;
+      const double *sf = v.sAcc + v.e * SA;
+      const int nfh = V::T::nf(v.h), f0h = V::T::f0(v.h);
+      const double *w1h = v.sW1 + R * L * f0h;
+      for (int s = 0; s < nfh; ++s) {
+        int ff = v.l + s;
+        if (ff >= nfh) ff -= nfh;
+        const int f = f0h + ff;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const double w = 2.0 * v.sW1[(r * NF + s) * L + v.l];
+          const double w = 2.0 * w1h[(r * nfh + s) * L + v.l];
 #pragma unroll
           for (int q = 0; q < Nf; ++q) acc[r][q] = fma(w, sf[q * NF + f], acc[r][q]);
         }
@@ -436,7 +451,8 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
         const int i = v.l + L * r;
         if (i < Nq) {
 #pragma unroll
-          for (int q = 0; q < Nf; ++q) rowbuf[q * Nq + i] += acc[r][q];  // full RHS row
+          for (int q = 0; q < Nf; ++q)  // full RHS row
+            rowbuf[q * Nq + i] = H == 2 ? rowbuf[q * Nq + i] + acc[r][q] : acc[r][q];
         }
       }
     }
