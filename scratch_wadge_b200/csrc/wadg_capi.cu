@@ -111,19 +111,19 @@ int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const doubl
                        const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
                        const double *Qf, double *rhsQ, double *rhsQf) {
   using C = VolPairsCfg<DIM, N, CURVED, W>;
-  static_assert(C::smem <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
+  static_assert(C::smem_vol <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
   auto kern = vol_pairs_kernel<DIM, N, CURVED, W>;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_vol);
     if (e != cudaSuccess) return cuda_check(e, "volume kernel smem attribute");
     attr = true;
   }
-  const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
+  const int per_sm = (int)((227 * 1024) / C::smem_vol) > 0 ? (int)((227 * 1024) / C::smem_vol) : 1;
   const int batches = (K + C::E - 1) / C::E;
   const int grid = batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
-  kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
-                                                  VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
+  kern<<<grid, C::threads, C::smem_vol, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
+                                                      VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
   return after_launch("volume kernel");
 }
 

@@ -33,6 +33,16 @@ template <int DIM, int N> struct Elem {
   static constexpr int NS = DIM + 4;      // rho, velocity, beta, log rho, log beta
 };
 
+// 8-byte asynchronous global -> shared copies (cp.async, sm_80 and later):
+// the copies of a block are in flight together, occupying no registers, while
+// the issuing threads go on computing; commit + wait completes them
+__device__ __forceinline__ void cp_async8(double *dst_smem, const double *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 struct Phys {
   double gamma;
   double gm1;     // gamma - 1

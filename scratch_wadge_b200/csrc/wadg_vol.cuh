@@ -68,6 +68,11 @@ struct VolPairsCfg {
   static constexpr size_t fixed = sizeof(double) * (size_t)(nD + 2 * nW + El::Nfaces * DIM);
   static constexpr size_t per_elem = sizeof(double) * (size_t)(SE + SA + SN);
   static constexpr size_t smem = fixed + E * per_elem;
+  // the volume kernel stages the next batch's face traces (cp.async) while it
+  // computes the current one, where shared memory has room for them
+  static constexpr size_t pre = sizeof(double) * (size_t)E * El::Nfields * El::NfqNf;
+  static constexpr bool PREFETCH = smem + pre <= 227 * 1024;
+  static constexpr size_t smem_vol = smem + (PREFETCH ? pre : 0);
 };
 
 // Shared-memory carve-up and the two phases common to both kernels.
@@ -80,7 +85,7 @@ struct VolPairs {
   static constexpr int Nf = El::Nfields, NG = El::Nvgeo, L = T::L, R = T::R, G = T::G, E = C::E;
   static constexpr int SE = C::SE, SA = C::SA, SN = C::SN, H = C::H;
 
-  double *sD, *sW1, *sW2, *sNr, *sSt, *sAcc, *sNrm;
+  double *sD, *sW1, *sW2, *sNr, *sSt, *sAcc, *sNrm, *sPre;
   int tid, h, g, l, e;
 
   __device__ __forceinline__ VolPairs(double *smem) {
@@ -91,6 +96,7 @@ struct VolPairs {
     sSt = sNr + El::Nfaces * DIM;  // [E][SE]     node states (+ geometric factors)
     sAcc = sSt + E * SE;           // [E][SA]     face-row accumulators
     sNrm = sAcc + E * SA;          // [E][SN]     per-face nJ (affine) + G
+    sPre = sNrm + E * SN;          // [E][Nf][NF] staged face traces (volume kernel, PREFETCH)
     tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     h = warp % H;
@@ -131,14 +137,17 @@ struct VolPairs {
   }
 
   // node states of the batch (one thread per node); elements past the end
-  // replicate the last element so that every lane computes on valid data
+  // replicate the last element so that every lane computes on valid data.
+  // ufs: the batch's face traces already staged in shared memory, or null
   __device__ __forceinline__ void prologue(int K, int k0, const double *vgeo, const double *vfgeo,
-                                           const double *uq, const double *uf, const Phys &P) {
+                                           const double *uq, const double *uf, const Phys &P,
+                                           const double *ufs = nullptr) {
     for (int t = tid; t < E * NN; t += blockDim.x) {
       const int ee = t / NN, n = t % NN;
       const int k = min(k0 + ee, K - 1);
+      const double *fsrc = ufs ? ufs + (size_t)(k - k0) * NF * Nf : uf + (size_t)k * NF * Nf;
       const NodeState<DIM> s = (n < Nq) ? node_state<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
-                                        : node_state<DIM>(uf + (size_t)k * NF * Nf + (n - Nq), NF, P);
+                                        : node_state<DIM>(fsrc + (n - Nq), NF, P);
       double *st = sSt + ee * SE;
       st[0 * NN + n] = s.rho;
 #pragma unroll
@@ -312,11 +321,24 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
   extern __shared__ double smem[];
   V v(smem);
   v.load_tables(nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq);
+  constexpr bool PRE = V::C::PREFETCH;
+  // stage batch kb's face traces (a contiguous range of Qf) into shared memory
+  auto prefetch = [&](int kb) {
+    if (kb < K) {
+      const int n = min(K - kb, E) * NF * Nf;
+      const double *src = Qf + (size_t)kb * NF * Nf;
+      for (int t = threadIdx.x; t < n; t += blockDim.x) cp_async8(v.sPre + t, src + t);
+    }
+    cp_async_commit();
+  };
+  if (PRE) prefetch(blockIdx.x * E);
 
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
-    __syncthreads();  // tables ready / previous batch done with shared memory
-    v.prologue(K, k0, vgeo, vfgeo, rhsQ, Qf, P);
+    if (PRE) cp_async_wait_all();
+    __syncthreads();  // tables ready / previous batch done with shared memory / traces staged
+    v.prologue(K, k0, vgeo, vfgeo, rhsQ, Qf, P, PRE ? v.sPre : nullptr);
     __syncthreads();
+    if (PRE) prefetch(k0 + gridDim.x * E);  // the next batch's traces, during the pairs
     double acc[R][Nf];
     v.pairs(acc, P);
     __syncthreads();  // all pairs done: the state block becomes the row buffer
