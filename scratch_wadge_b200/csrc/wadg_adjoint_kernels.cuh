@@ -389,7 +389,12 @@ struct AdjPairsCfg {
   static constexpr int nTD = DIM * R * Nq * L;
   static constexpr int nTW = R * NF * L;
   static constexpr size_t fixed = sizeof(double) * (size_t)(nTD + 2 * nTW + El::Nfaces * DIM);
-  static constexpr size_t smem = fixed + sizeof(double) * (size_t)E * per_elem;
+  static constexpr size_t smem_core = fixed + sizeof(double) * (size_t)E * per_elem;
+  // the next batch's face traces are staged (cp.async) during the pair phase
+  // where shared memory has room for them
+  static constexpr size_t pre = sizeof(double) * (size_t)E * Nf * NF;
+  static constexpr bool PREFETCH = smem_core + pre <= 227 * 1024;
+  static constexpr size_t smem = smem_core + (PREFETCH ? pre : 0);
   static_assert(W % H == 0, "warps per CTA must be a multiple of the warps per element");
 };
 
@@ -415,6 +420,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
   double *tW2 = tW1 + C::nTW;        // [h][r][s][l] -1/2 VfPq(f, i)
   double *sNr = tW2 + C::nTW;        // [Nfaces][DIM]
   double *sEl = sNr + El::Nfaces * DIM;
+  double *sPre = sEl + E * C::per_elem;  // [E][Nf][NF] staged face traces (PREFETCH)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int h = warp % H, g = lane / L, l = lane % L;
@@ -464,14 +470,27 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
   const double *tW1h = tW1 + R * L * cf(h), *tW2h = tW2 + R * L * cf(h);
   const adj::Gas gas = gas_of(P);
 
+  constexpr bool PRE = C::PREFETCH;
+  auto prefetch = [&](int kb) {
+    if (kb < K) {
+      const int n = min(K - kb, E) * NF * Nf;
+      const double *src = uf + (size_t)kb * NF * Nf;
+      for (int t = tid; t < n; t += blockDim.x) cp_async8(sPre + t, src + t);
+    }
+    cp_async_commit();
+  };
+  if (PRE) prefetch(blockIdx.x * E);
+
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
-    __syncthreads();  // tables ready / previous batch done with shared memory
+    if (PRE) cp_async_wait_all();
+    __syncthreads();  // tables ready / previous batch done with shared memory / traces staged
     // ---- prologue: node states, face seeds, zeroed column adjoints, normals
     for (int t = tid; t < E * NN; t += blockDim.x) {
       const int ee = t / NN, n = t % NN;
       const int k = min(k0 + ee, K - 1);
+      const double *fsrc = PRE ? sPre + (size_t)(k - k0) * NF * Nf : uf + (size_t)k * NF * Nf;
       const AdjNode<DIM> s = (n < Nq) ? adj_node<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
-                                      : adj_node<DIM>(uf + (size_t)k * NF * Nf + (n - Nq), NF, P);
+                                      : adj_node<DIM>(fsrc + (n - Nq), NF, P);
       double *st = sEl + ee * C::per_elem;
       st[0 * NN + n] = s.rho;
 #pragma unroll
@@ -517,6 +536,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
       }
     }
     __syncthreads();
+    if (PRE) prefetch(k0 + gridDim.x * E);  // the next batch's traces, during the pairs
 
     // ---- pairs
     const double *st = sEl + e * C::per_elem;
