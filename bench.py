@@ -425,7 +425,7 @@ def run_adjoint_measurement(nhex=8, nsteps=200, every=20, reps=3, fd_dirs=2):
 
 
 def run_ensemble_measurement(steps=5, warmup=2):
-    """256 independent 2D vortex solves (K log-uniform in
+    """The batched-ensemble workload: 256 independent 2D vortex solves (K log-uniform in
     [200, 8192], N uniform in {2,3,4}, seeded), batched (bins + one CUDA graph
     per time step) against the plain one-instance-per-launch path, same dt and
     steps; throughput in DOF*stages/s, timed with CUDA events."""
