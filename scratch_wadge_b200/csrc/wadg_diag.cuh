@@ -1,4 +1,4 @@
-// Per-element diagnostics (§a12 of the hot-path table): the kinetic energy of
+// Per-element diagnostics: the kinetic energy of
 // euler_3d_compute_aux (Euler3D.okl:3888-3934) and the entropy integral the
 // reference's driver sums on the host (euler.c:4135-4156, 4276-4315).
 //   KE_k = sum_i 1/2 |m_i|^2 / rho_i  J_ik w_i
