@@ -66,6 +66,16 @@ __device__ __forceinline__ double rcp(double x) {
   return y;
 }
 
+// 1/x with one Newton-Raphson step: relative error ~1e-14, for quantities
+// that only feed a series argument or a branch test (the log-mean's u), never
+// a result directly.
+__device__ __forceinline__ double rcp1(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
 // Log-mean of a, b > 0: (a - b) / (log a - log b).
 //
 // The reference (Euler3Daffine.okl:43-71, Euler2D.okl:36-67) evaluates
@@ -238,7 +248,10 @@ __device__ __forceinline__ void ecflux_n_warp(const NodeState<DIM> &a, const Nod
                                               const double *n, const Phys &P, double *F) {
   const double sr = a.rho + b.rho, dr = a.rho - b.rho;
   const double sb = a.beta + b.beta, db = a.beta - b.beta;
-  const double isr = rcp(sr), isb = rcp(sb);
+  // 1/(a+b) of the densities only forms the series argument ur (and its
+  // branch test): one Newton step suffices; 1/(a+b) of beta enters pa and the
+  // mean itself, so it gets two
+  const double isr = rcp1(sr), isb = rcp(sb);
   const double fr = dr * isr, fb = db * isb;
   const double ur = fr * fr, ub = fb * fb;
   double rl, ibl;
