@@ -278,6 +278,43 @@ __device__ __forceinline__ void ecflux_n_warp(const NodeState<DIM> &a, const Nod
   F[DIM + 1] = f4 * un;
 }
 
+// ecflux_n_warp for states whose velocity is stored halved (vel = u/2), the
+// pair kernel's layout: ubar = a.vel + b.vel, (ua.ub)/2 = 2 (a.vel . b.vel),
+// and (rho_a + rho_b)/2 is formed once for rholog and pa.  Same value to
+// rounding.  Must be called by all 32 lanes of the warp.
+template <int DIM>
+__device__ __forceinline__ void ecflux_n_warp_h(const NodeState<DIM> &a, const NodeState<DIM> &b,
+                                                const double *n, const Phys &P, double *F) {
+  const double sr = a.rho + b.rho, dr = a.rho - b.rho;
+  const double sb = a.beta + b.beta, db = a.beta - b.beta;
+  const double isr = rcp1(sr), isb = rcp(sb);
+  const double fr = dr * isr, fb = db * isb;
+  const double ur = fr * fr, ub = fb * fb;
+  const double hsr = 0.5 * sr;
+  double rl, ibl;
+  if (__all_sync(0xffffffffu, fmax(ur, ub) < 1e-6)) {
+    rl = hsr * polyG2(ur);
+    ibl = 2.0 * isb * polyF2(ub);
+  } else {
+    rl = (ur < 1e-2) ? hsr * polyG(ur) : dr * rcp(a.lrho - b.lrho);
+    ibl = (ub < 1e-2) ? 2.0 * isb * polyF(ub) : (a.lbeta - b.lbeta) * rcp(db);
+  }
+  const double pa = hsr * isb;
+  double ubar[DIM], un = 0.0, hv = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    ubar[d] = a.vel[d] + b.vel[d];
+    un = fma(ubar[d], n[d], un);
+    hv = fma(a.vel[d], b.vel[d], hv);
+  }
+  const double f4 = fma(rl, fma(ibl, P.cbeta, 2.0 * hv), pa);
+  const double F0 = rl * un;
+  F[0] = F0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) F[1 + d] = fma(F0, ubar[d], pa * n[d]);
+  F[DIM + 1] = f4 * un;
+}
+
 }  // namespace wadg
 
 namespace wadg {

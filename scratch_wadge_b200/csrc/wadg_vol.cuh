@@ -151,7 +151,7 @@ struct VolPairs {
       double *st = sSt + ee * SE;
       st[0 * NN + n] = s.rho;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = s.vel[d];
+      for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = 0.5 * s.vel[d];  // stored halved
       st[(DIM + 1) * NN + n] = s.beta;
       st[(DIM + 2) * NN + n] = s.lrho;
       st[(DIM + 3) * NN + n] = s.lbeta;
@@ -184,6 +184,7 @@ struct VolPairs {
     }
   }
 
+  // a node's state as the pair phase keeps it: velocity stored halved (u/2)
   __device__ __forceinline__ NodeState<DIM> load(const double *st, int n) const {
     NodeState<DIM> s;
     s.rho = st[n];
@@ -237,7 +238,7 @@ struct VolPairs {
           }
           nv[d] = v;
         }
-        ecflux_n_warp<DIM>(A[r], B, nv, P, F);
+        ecflux_n_warp_h<DIM>(A[r], B, nv, P, F);
 #pragma unroll
         for (int q = 0; q < Nf; ++q) acc[r][q] += F[q];
       }
@@ -275,7 +276,7 @@ struct VolPairs {
           }
         }
         double F[Nf];
-        ecflux_n_warp<DIM>(A[r], B, nv, P, F);
+        ecflux_n_warp_h<DIM>(A[r], B, nv, P, F);
         const double w1 = w1h[(r * nfh + s) * L + l];
         const double w2 = w2h[(r * nfh + s) * L + l];
 #pragma unroll
@@ -423,7 +424,9 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
         UM[q] = uf[idM + q * NF];
         UP[q] = uf[idP + q * NF];
       }
-      const NodeState<DIM> M = v.load(v.sSt + ee * SE, Nq + f);
+      NodeState<DIM> M = v.load(v.sSt + ee * SE, Nq + f);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) M.vel[d] *= 2.0;  // the pair phase's states hold u/2
       const NodeState<DIM> Pp = node_state_nolog<DIM>(UP, 1, P);
       double F[Nf];
       ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
