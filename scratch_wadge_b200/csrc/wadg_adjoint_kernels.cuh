@@ -108,7 +108,7 @@ __device__ __forceinline__ FluxCore<DIM> flux_core(const AdjNode<DIM> &a, const 
   FluxCore<DIM> k;
   const double sr = a.rho + b.rho, dr = a.rho - b.rho;
   const double sb = a.beta + b.beta, db = a.beta - b.beta;
-  const double isr = rcp(sr);
+  const double isr = rcp1(sr);  // forms only the series argument and f(1 -+ f)
   k.isb = rcp(sb);
   const double fr = dr * isr, fb = db * k.isb;
   const double ur = fr * fr, ub = fb * fb;
