@@ -13,6 +13,7 @@
 #include "../../include/wadg.h"
 #include "wadg_diag.cuh"
 #include "wadg_kernels.cuh"
+#include "wadg_update_mma.cuh"
 #include "wadg_vol.cuh"
 
 using namespace wadg;
@@ -54,7 +55,6 @@ template <int DIM, int N> constexpr int volE() { return pickE(320, Elem<DIM, N>:
 template <int DIM, int N> constexpr int surfE() {
   return pickE(128, Elem<DIM, N>::NfqNf > Elem<DIM, N>::Nq ? Elem<DIM, N>::NfqNf : Elem<DIM, N>::Nq);
 }
-template <int DIM, int N> constexpr int updE() { return pickE(256, Elem<DIM, N>::Nq); }
 
 template <int DIM, int N, bool CURVED>
 int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
@@ -192,11 +192,21 @@ template <int DIM, int N, bool CURVED>
 int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq,
                   const double *VfPq, double fa, double fb, double fdt, double *rhsQ,
                   double *resQ, double *Q, double *Qf) {
-  constexpr int E = updE<DIM, N>();
-  using C = UpdCfg<DIM, N, CURVED, E>;
-  const int grid = (K + E - 1) / E;
-  update_kernel<DIM, N, CURVED, E><<<grid, C::threads, C::smem, c->stream>>>(
-      K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf, c->phys);
+  using C = UpdMmaCfg<DIM, N, CURVED>;
+  static_assert(C::smem <= 227 * 1024, "update kernel does not fit in shared memory");
+  auto kern = update_mma_kernel<DIM, N, CURVED>;
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    if (e != cudaSuccess) return cuda_check(e, "update kernel smem attribute");
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::threads, C::smem);
+    if (e != cudaSuccess) return cuda_check(e, "update kernel occupancy");
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int ctas = (K + C::EW - 1) / C::EW;
+  const int grid = ctas < num_sms() * per_sm ? ctas : num_sms() * per_sm;
+  kern<<<grid, C::threads, C::smem, c->stream>>>(K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q,
+                                                 Qf, c->phys);
   return after_launch("update kernel");
 }
 

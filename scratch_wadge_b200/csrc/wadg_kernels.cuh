@@ -1,4 +1,5 @@
-// The three kernels of one LSRK stage (volume, surface, update), templated on
+// The row-per-thread volume kernel and the surface kernel of one LSRK stage (the
+// update kernel is in wadg_update_mma.cuh), templated on
 // dimension and degree.  One CTA handles E consecutive elements; everything an
 // element reads more than once is staged in shared memory.
 #pragma once
@@ -241,138 +242,6 @@ surf_kernel(int K, const double *__restrict__ fgeo, const uint32_t *__restrict__
     double *out = rhsQ + (size_t)k * Nq * Nf + i;
 #pragma unroll
     for (int f = 0; f < Nf; ++f) out[f * Nq] += val[f];
-  }
-}
-
-// ---------------------------------------------------------------- update
-// affine (Euler3Daffine.okl:555-773, Euler2D.okl:1498-1725):
-//   r = -2 VqPq rhs / J; res = a res + dt r; Q += b res; v = V(Q);
-//   Qf = U(VfPq v); rhsQ = U(VqPq v)
-// WADG (Euler3D.okl:2527-2884, Euler2D.okl:1729-2282):
-//   r = VqPq((-2 VqPq rhs)/J); ...; v~ = VqPq((VqPq(v J))/J);
-//   Qf = U(VfPq v~); rhsQ = U(VqPq v~)
-template <int DIM, int N, bool CURVED, int E>
-struct UpdCfg {
-  using El = Elem<DIM, N>;
-  static constexpr int threads = E * El::Nq;
-  static constexpr size_t smem = sizeof(double) * 2 * E * El::Nfields * El::Nq;
-};
-
-template <int DIM, int N, bool CURVED, int E>
-__global__ void __launch_bounds__(UpdCfg<DIM, N, CURVED, E>::threads)
-update_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
-              const double *__restrict__ VfPq, double fa, double fb, double fdt,
-              double *__restrict__ rhsQ, double *__restrict__ resQ, double *__restrict__ Q,
-              double *__restrict__ Qf, Phys P) {
-  using El = Elem<DIM, N>;
-  constexpr int Nq = El::Nq, NfqNf = El::NfqNf, Nf = El::Nfields;
-  extern __shared__ double smem[];
-  double (*s)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
-  double (*sV)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
-  const int k0 = blockIdx.x * E;
-  const int kend = min(K - k0, E);
-
-  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
-  const bool valid = e < kend;
-  const size_t id = (size_t)k * Nq * Nf + i;
-  // this thread's LSRK operands, loaded first so that their latency overlaps
-  // the staging of the RHS block
-  double res0[Nf], q0[Nf];
-  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
-  if (valid) {
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) {
-      res0[f] = resQ[id + f * Nq];
-      q0[f] = Q[id + f * Nq];
-    }
-  }
-
-  // the E elements' rhsQ blocks are one contiguous range: copy it flat
-  const double *src = rhsQ + (size_t)k0 * Nf * Nq;
-  for (int t = threadIdx.x; t < kend * Nf * Nq; t += blockDim.x) (&s[0][0][0])[t] = src[t];
-  __syncthreads();
-
-  auto matvec = [&](const double *Op, int ld, int row, double (*X)[Nq], double *out) {
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) out[f] = 0.0;
-    for (int j = 0; j < Nq; ++j) {
-      const double w = __ldg(Op + row + j * ld);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) out[f] = fma(w, X[f][j], out[f]);
-    }
-  };
-
-  double r[Nf];
-  if (CURVED) {
-    if (valid) {
-      matvec(VqPq, Nq, i, s[e], r);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) sV[e][f][i] = -2.0 * r[f] / Jqi;
-    }
-    __syncthreads();
-    if (valid) matvec(VqPq, Nq, i, sV[e], r);
-  } else if (valid) {
-    matvec(VqPq, Nq, i, s[e], r);
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) r[f] = -2.0 * r[f] / Jqi;
-  }
-
-  double V[Nf];
-  if (valid) {
-    double U[Nf];
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) {
-      const double res = fa * res0[f] + fdt * r[f];
-      resQ[id + f * Nq] = res;
-      U[f] = q0[f] + fb * res;
-      Q[id + f * Nq] = U[f];
-    }
-    VU<DIM>(U, V, P);
-  }
-
-  double (*X)[Nf][Nq] = sV;  // what the final projection reads
-  if (CURVED) {
-    __syncthreads();  // everyone is done reading s (first matvec)
-    if (valid)
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) s[e][f][i] = V[f] * Jqi;
-    __syncthreads();
-    if (valid) {
-      matvec(VqPq, Nq, i, s[e], r);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) sV[e][f][i] = r[f] / Jqi;
-    }
-    __syncthreads();
-    if (valid) matvec(VqPq, Nq, i, sV[e], r);
-    __syncthreads();
-    if (valid)
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) s[e][f][i] = r[f];
-    X = s;
-  } else {
-    if (valid)
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) sV[e][f][i] = V[f];
-  }
-  __syncthreads();
-
-  // face and volume outputs spread evenly over the CTA's threads
-  for (int t = threadIdx.x; t < kend * (NfqNf + Nq); t += blockDim.x) {
-    const int ee = t / (NfqNf + Nq), n = t % (NfqNf + Nq), kk = k0 + ee;
-    double Vv[Nf], Uu[Nf];
-    if (n < NfqNf) {
-      matvec(VfPq, NfqNf, n, X[ee], Vv);
-      UV<DIM>(Vv, Uu, P);
-      double *out = Qf + (size_t)kk * NfqNf * Nf + n;
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) out[f * NfqNf] = Uu[f];
-    } else {
-      matvec(VqPq, Nq, n - NfqNf, X[ee], Vv);
-      UV<DIM>(Vv, Uu, P);
-      double *out = rhsQ + (size_t)kk * Nq * Nf + (n - NfqNf);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) out[f * Nq] = Uu[f];
-    }
   }
 }
 

@@ -1,0 +1,298 @@
+// LSRK update kernel (wadg_euler_update_*) with its projections on the FP64
+// tensor cores.  Same arithmetic as the reference's update kernels
+// (Euler3Daffine.okl:555-773, Euler3D.okl:2527-2884, Euler2D.okl:1498-2282):
+//   affine: r = -2 VqPq rhs / J; res = a res + dt r; Q += b res; v = V(Q);
+//           Qf = U(VfPq v); rhsQ = U(VqPq v)
+//   WADG:   r = VqPq((-2 VqPq rhs)/J); ...; v~ = VqPq((VqPq(v J))/J);
+//           Qf = U(VfPq v~); rhsQ = U(VqPq v~)
+// but every operator application is a small GEMM over a group of 8 elements,
+// Op[M x Nq] * X[Nq x (8 Nf)], issued as mma.sync m8n8k4 f64 (the FP64 MMA of
+// sm_80 and later; tcgen05 has no f64 kind).  A node-per-thread matrix-vector
+// product issues one shared-memory load per FMA and is bound by the LSU pipe;
+// a fragment-tiled MMA loads one B value per 8 FMAs.
+//
+// One CTA works on one group of 8 elements at a time:
+//   * the group's rhs block is staged in shared memory as X[node][f*8 + e]
+//     (column n of the GEMM = field f of element e), so that one n-tile of 8
+//     columns is one field of the 8 elements;
+//   * a warp computes all Nf n-tiles of an m-tile of 8 output nodes (the
+//     CTA's warps take the m-tiles round-robin), so a lane
+//     ends up holding every field of its (node, element) pairs in registers —
+//     the nonlinear epilogues (V(U), U(V), the LSRK update) run there, with no
+//     round trip through shared memory;
+//   * rows of X beyond Nq are zero and the operator's fragments beyond its
+//     extent are zero, so the padding adds nothing.
+// The row stride of X is = 4 or 12 (mod 16) doubles: a half warp's B-fragment
+// load (4 k-rows x 4 columns) then hits 16 distinct banks.
+#pragma once
+
+#include "wadg_device.cuh"
+
+namespace wadg {
+
+// D(8x8) += A(8x4) B(4x8).  Lane l holds A(l/4, l%4), B(l%4, l/4) and
+// D(l/4, 2(l%4)), D(l/4, 2(l%4)+1).
+// (not volatile: independent MMAs may be interleaved by the scheduler)
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+constexpr int mma_ld(int c) { return (c % 16 == 4 || c % 16 == 12) ? c : mma_ld(c + 1); }
+
+template <int DIM, int N, bool CURVED>
+struct UpdMmaCfg {
+  using El = Elem<DIM, N>;
+  static constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
+  static constexpr int EW = 8;                      // elements per warp (one n-tile per field)
+  static constexpr int KS = (Nq + 3) / 4;           // k-steps of 4 nodes
+  static constexpr int KP = 4 * KS;                 // rows of X (zero beyond Nq)
+  static constexpr int MQ = (Nq + 7) / 8;           // m-tiles of the Nq x Nq products
+  static constexpr int MO = (NF + Nq + 7) / 8;      // m-tiles of [VfPq; VqPq]
+  static constexpr int LD = mma_ld(Nf * EW);        // row stride of X (doubles)
+  static constexpr int BUF = KP * LD;               // one buffer
+  // one CTA works on one group at a time, one warp per m-tile of the Nq x Nq
+  // products (the output projection's MO m-tiles go round-robin)
+  static constexpr int WARPS = MQ < 2 ? 2 : (MQ > 6 ? 6 : MQ);
+  static constexpr int threads = 32 * WARPS;
+  static constexpr size_t smem = sizeof(double) * 2 * BUF;
+};
+
+// A fragments of rows [8 mt, 8 mt + 8) of an operator stored column-major
+// (Op(m, k) = Op[m + k ld], rows < M, columns < Nq); zero outside
+template <int KS, int Nq>
+__device__ __forceinline__ void load_afrag(const double *__restrict__ Op, int ld, int M, int mt,
+                                           int lane, double *a) {
+  const int m = mt * 8 + (lane >> 2);
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    const int k = ks * 4 + (lane & 3);
+    a[ks] = (m < M && k < Nq) ? __ldg(Op + m + (size_t)k * ld) : 0.0;
+  }
+}
+
+// the stacked operator [VfPq; VqPq] (NF + Nq rows)
+template <int KS, int Nq, int NF>
+__device__ __forceinline__ void load_afrag_out(const double *__restrict__ VfPq,
+                                               const double *__restrict__ VqPq, int mt, int lane,
+                                               double *a) {
+  const int m = mt * 8 + (lane >> 2);
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    const int k = ks * 4 + (lane & 3);
+    double v = 0.0;
+    if (k < Nq) {
+      if (m < NF)
+        v = __ldg(VfPq + m + (size_t)k * NF);
+      else if (m < NF + Nq)
+        v = __ldg(VqPq + (m - NF) + (size_t)k * Nq);
+    }
+    a[ks] = v;
+  }
+}
+
+// D[f][i] = sum_k A(m, k) X(k, f*8 + e), m = 8 mt + lane/4, e = 2 (lane%4) + i
+template <int KS, int Nf, int LD>
+__device__ __forceinline__ void mtile_gemm(const double *a, const double *X, int lane,
+                                           double (*D)[2]) {
+  const double *xb = X + (lane & 3) * LD + (lane >> 2);
+#pragma unroll
+  for (int f = 0; f < Nf; ++f) D[f][0] = D[f][1] = 0.0;
+  // k outer: the Nf accumulator chains are independent, so consecutive MMAs
+  // do not wait on each other
+#pragma unroll
+  for (int ks = 0; ks < KS; ++ks) {
+    double b[Nf];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) b[f] = xb[ks * 4 * LD + f * 8];
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) dmma884(D[f][0], D[f][1], a[ks], b[f]);
+  }
+}
+
+// Y(m, f*8 + e) = c D[f][i] / J(m, e) for the lane's rows < Nq (J = 1
+// without a Jacobian; columns of elements past the end get 0)
+template <int Nq, int Nf, int LD, bool DIVJ>
+__device__ __forceinline__ void mtile_store(double *Y, int mt, int lane, const double (*D)[2],
+                                            double c, const double *__restrict__ Jq, int k0,
+                                            int ne) {
+  const int m = mt * 8 + (lane >> 2);
+  if (m >= Nq) return;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int e = 2 * (lane & 3) + i;
+    const bool ok = e < ne;
+    const double J = (DIVJ && ok) ? Jq[(size_t)(k0 + e) * Nq + m] : 1.0;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) Y[m * LD + f * 8 + e] = ok ? (DIVJ ? c * D[f][i] / J : D[f][i]) : 0.0;
+  }
+}
+
+// the LSRK operands of a lane's two (node, element) pairs of m-tile mt
+template <int Nq, int Nf>
+__device__ __forceinline__ void load_lsrk(const double *__restrict__ resQ,
+                                          const double *__restrict__ Q,
+                                          const double *__restrict__ Jq, int k0, int ne, int mt,
+                                          int lane, double (*res0)[Nf], double (*q0)[Nf],
+                                          double *Jv) {
+  const int m = mt * 8 + (lane >> 2);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int e = 2 * (lane & 3) + i;
+    const bool ok = m < Nq && e < ne;
+    const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
+    Jv[i] = ok ? Jq[(size_t)(k0 + e) * Nq + m] : 1.0;
+#pragma unroll
+    for (int f = 0; f < Nf; ++f) {
+      res0[i][f] = ok ? resQ[id + f * Nq] : 0.0;
+      q0[i][f] = ok ? Q[id + f * Nq] : 1.0;
+    }
+  }
+}
+
+template <int DIM, int N, bool CURVED>
+__global__ void __launch_bounds__(UpdMmaCfg<DIM, N, CURVED>::threads)
+update_mma_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
+                  const double *__restrict__ VfPq, double fa, double fb, double fdt,
+                  double *__restrict__ rhsQ, double *__restrict__ resQ, double *__restrict__ Q,
+                  double *__restrict__ Qf, Phys P) {
+  using C = UpdMmaCfg<DIM, N, CURVED>;
+  constexpr int Nq = C::Nq, NF = C::NF, Nf = C::Nf, EW = C::EW, KS = C::KS, KP = C::KP,
+                LD = C::LD, MQ = C::MQ, MO = C::MO, W = C::WARPS;
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *X = smem;
+  double *Y = X + C::BUF;
+  // the padding rows stay zero for the whole launch
+  for (int t = threadIdx.x; t < (KP - Nq) * LD; t += C::threads) {
+    X[Nq * LD + t] = 0.0;
+    Y[Nq * LD + t] = 0.0;
+  }
+
+  const int ngroups = (K + EW - 1) / EW;
+  for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    const int k0 = g * EW;
+    const int ne = min(EW, K - k0);
+    bool ev[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) ev[i] = 2 * (lane & 3) + i < ne;
+
+    // ---- stage the group's rhs block [e][f][node] as X[node][f*8 + e]; the
+    // LSRK operands of this warp's first m-tile are loaded alongside
+    constexpr int TOT = EW * Nf * Nq, IT = (TOT + C::threads - 1) / C::threads;
+    double res0[2][Nf], q0[2][Nf], Jv[2];
+    {
+      const double *src = rhsQ + (size_t)k0 * Nf * Nq;
+      const int lim = ne * Nf * Nq;
+      double v[IT];
+#pragma unroll
+      for (int it = 0; it < IT; ++it) {
+        const int t = threadIdx.x + C::threads * it;
+        v[it] = t < lim ? src[t] : 0.0;
+      }
+      if (warp < MQ) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, warp, lane, res0, q0, Jv);
+      __syncthreads();  // the previous group's last reads of X and Y are done
+#pragma unroll
+      for (int it = 0; it < IT; ++it) {
+        const int t = threadIdx.x + C::threads * it;
+        if (t < TOT) {
+          const int e = t / (Nf * Nq), rem = t - e * (Nf * Nq);
+          const int f = rem / Nq, n = rem - f * Nq;
+          X[n * LD + f * EW + e] = v[it];
+        }
+      }
+    }
+    __syncthreads();
+
+    double a[KS], D[Nf][2];
+    // ---- r = M^{-1} rhs (affine: -2 VqPq rhs / J; WADG: VqPq(-2 VqPq rhs / J))
+    const double *R = X;  // the operand of the last product before the update
+    if (CURVED) {
+      for (int mt = warp; mt < MQ; mt += W) {
+        load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+        mtile_gemm<KS, Nf, LD>(a, X, lane, D);
+        mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, -2.0, Jq, k0, ne);
+      }
+      __syncthreads();
+      R = Y;
+    }
+    // the update proper; V(U) goes to the other buffer (affine: Y; WADG: X,
+    // scaled by J for the projection that follows)
+    double *Vb = CURVED ? X : Y;
+    for (int mt = warp; mt < MQ; mt += W) {
+      if (mt != warp) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, mt, lane, res0, q0, Jv);
+      const int m = mt * 8 + (lane >> 2);
+      load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+      mtile_gemm<KS, Nf, LD>(a, R, lane, D);
+      if (m < Nq) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int e = 2 * (lane & 3) + i;
+          const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
+          double U[Nf], V[Nf];
+#pragma unroll
+          for (int f = 0; f < Nf; ++f) {
+            const double r = CURVED ? D[f][i] : -2.0 * D[f][i] / Jv[i];
+            const double res = fa * res0[i][f] + fdt * r;
+            U[f] = q0[i][f] + fb * res;
+            if (ev[i]) {
+              resQ[id + f * Nq] = res;
+              Q[id + f * Nq] = U[f];
+            }
+          }
+          if (ev[i]) {
+            VU<DIM>(U, V, P);
+          } else {
+#pragma unroll
+            for (int f = 0; f < Nf; ++f) V[f] = 0.0;
+          }
+#pragma unroll
+          for (int f = 0; f < Nf; ++f) Vb[m * LD + f * EW + e] = CURVED ? V[f] * Jv[i] : V[f];
+        }
+      }
+    }
+    __syncthreads();
+    const double *Xo = Y;  // the operand of the output projection
+    if (CURVED) {
+      // v~ = VqPq((VqPq(v J)) / J): X -> Y -> X
+      for (int mt = warp; mt < MQ; mt += W) {
+        load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+        mtile_gemm<KS, Nf, LD>(a, X, lane, D);
+        mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, 1.0, Jq, k0, ne);
+      }
+      __syncthreads();
+      for (int mt = warp; mt < MQ; mt += W) {
+        load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+        mtile_gemm<KS, Nf, LD>(a, Y, lane, D);
+        mtile_store<Nq, Nf, LD, false>(X, mt, lane, D, 1.0, Jq, k0, ne);
+      }
+      __syncthreads();
+      Xo = X;
+    }
+
+    // ---- Qf = U(VfPq v), rhsQ = U(VqPq v)
+    for (int mt = warp; mt < MO; mt += W) {
+      load_afrag_out<KS, Nq, NF>(VfPq, VqPq, mt, lane, a);
+      mtile_gemm<KS, Nf, LD>(a, Xo, lane, D);
+      const int m = mt * 8 + (lane >> 2);
+      if (m >= NF + Nq) continue;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        if (!ev[i]) continue;
+        const int e = 2 * (lane & 3) + i;
+        double V[Nf], U[Nf];
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) V[f] = D[f][i];
+        UV<DIM>(V, U, P);
+        double *out = m < NF ? Qf + (size_t)(k0 + e) * NF * Nf + m
+                             : rhsQ + (size_t)(k0 + e) * Nq * Nf + (m - NF);
+        const int ld = m < NF ? NF : Nq;
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) out[f * ld] = U[f];
+      }
+    }
+  }
+}
+
+}  // namespace wadg
