@@ -57,6 +57,10 @@ struct UpdMmaCfg {
   static constexpr int WARPS = MQ < 2 ? 2 : (MQ > 6 ? 6 : MQ);
   static constexpr int threads = 32 * WARPS;
   static constexpr size_t smem = sizeof(double) * 2 * BUF;
+  // register cap from the launch bounds: 5 resident CTAs per SM measured best
+  // (3D N=3 affine: 0.065 ms vs 0.067 uncapped and 0.065 at 7; the
+  // latency of the per-group chain wants warps more than registers)
+  static constexpr int min_ctas = 5;
 };
 
 // A fragments of rows [8 mt, 8 mt + 8) of an operator stored column-major
@@ -151,15 +155,152 @@ __device__ __forceinline__ void load_lsrk(const double *__restrict__ resQ,
   }
 }
 
+// The update of one group once X holds its RHS (rows < Nq; rows beyond are
+// zero): r = M^{-1} rhs, the LSRK update of resQ and Q, v = V(Q) (WADG: the
+// weight-adjusted projection of v), the next traces U(VfPq v) -> Qf_out and
+// U(VqPq v) -> rhsQ_out.  res0/q0/Jv hold the LSRK operands of the warp's
+// first m-tile (load_lsrk), loaded early by the caller.  Every warp of the
+// CTA calls this; it ends with the output stores (the caller synchronises
+// before X or Y are written again).
 template <int DIM, int N, bool CURVED>
-__global__ void __launch_bounds__(UpdMmaCfg<DIM, N, CURVED>::threads)
+__device__ __forceinline__ void update_group(
+    int k0, int ne, int warp, int lane, double *X, double *Y, const double *__restrict__ Jq,
+    const double *__restrict__ VqPq, const double *__restrict__ VfPq, double fa, double fb,
+    double fdt, double *__restrict__ resQ, double *__restrict__ Q, double *__restrict__ rhsQ_out,
+    double *__restrict__ Qf_out, const Phys &P, double (*res0)[DIM + 2], double (*q0)[DIM + 2],
+    double *Jv) {
+  using C = UpdMmaCfg<DIM, N, CURVED>;
+  constexpr int Nq = C::Nq, NF = C::NF, Nf = C::Nf, EW = C::EW, KS = C::KS, LD = C::LD,
+                MQ = C::MQ, MO = C::MO, W = C::WARPS;
+  bool ev[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) ev[i] = 2 * (lane & 3) + i < ne;
+
+  double a[KS], D[Nf][2];
+  // ---- r = M^{-1} rhs (affine: -2 VqPq rhs / J; WADG: VqPq(-2 VqPq rhs / J))
+  const double *R = X;  // the operand of the last product before the update
+  if (CURVED) {
+    for (int mt = warp; mt < MQ; mt += W) {
+      load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+      mtile_gemm<KS, Nf, LD>(a, X, lane, D);
+      mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, -2.0, Jq, k0, ne);
+    }
+    __syncthreads();
+    R = Y;
+  }
+  // the update proper; V(U) goes to the other buffer (affine: Y; WADG: X,
+  // scaled by J for the projection that follows)
+  double *Vb = CURVED ? X : Y;
+  for (int mt = warp; mt < MQ; mt += W) {
+    if (mt != warp) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, mt, lane, res0, q0, Jv);
+    const int m = mt * 8 + (lane >> 2);
+    load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+    mtile_gemm<KS, Nf, LD>(a, R, lane, D);
+    if (m < Nq) {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int e = 2 * (lane & 3) + i;
+        const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
+        double U[Nf], V[Nf];
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) {
+          const double r = CURVED ? D[f][i] : -2.0 * D[f][i] / Jv[i];
+          const double res = fa * res0[i][f] + fdt * r;
+          U[f] = q0[i][f] + fb * res;
+          if (ev[i]) {
+            resQ[id + f * Nq] = res;
+            Q[id + f * Nq] = U[f];
+          }
+        }
+        if (ev[i]) {
+          VU<DIM>(U, V, P);
+        } else {
+#pragma unroll
+          for (int f = 0; f < Nf; ++f) V[f] = 0.0;
+        }
+#pragma unroll
+        for (int f = 0; f < Nf; ++f) Vb[m * LD + f * EW + e] = CURVED ? V[f] * Jv[i] : V[f];
+      }
+    }
+  }
+  __syncthreads();
+  const double *Xo = Y;  // the operand of the output projection
+  if (CURVED) {
+    // v~ = VqPq((VqPq(v J)) / J): X -> Y -> X
+    for (int mt = warp; mt < MQ; mt += W) {
+      load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+      mtile_gemm<KS, Nf, LD>(a, X, lane, D);
+      mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, 1.0, Jq, k0, ne);
+    }
+    __syncthreads();
+    for (int mt = warp; mt < MQ; mt += W) {
+      load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
+      mtile_gemm<KS, Nf, LD>(a, Y, lane, D);
+      mtile_store<Nq, Nf, LD, false>(X, mt, lane, D, 1.0, Jq, k0, ne);
+    }
+    __syncthreads();
+    Xo = X;
+  }
+
+  // ---- Qf = U(VfPq v), rhsQ = U(VqPq v)
+  for (int mt = warp; mt < MO; mt += W) {
+    load_afrag_out<KS, Nq, NF>(VfPq, VqPq, mt, lane, a);
+    mtile_gemm<KS, Nf, LD>(a, Xo, lane, D);
+    const int m = mt * 8 + (lane >> 2);
+    if (m >= NF + Nq) continue;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      if (!ev[i]) continue;
+      const int e = 2 * (lane & 3) + i;
+      double V[Nf], U[Nf];
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) V[f] = D[f][i];
+      UV<DIM>(V, U, P);
+      double *out = m < NF ? Qf_out + (size_t)(k0 + e) * NF * Nf + m
+                           : rhsQ_out + (size_t)(k0 + e) * Nq * Nf + (m - NF);
+      const int ld = m < NF ? NF : Nq;
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) out[f * ld] = U[f];
+    }
+  }
+}
+
+// stage the rhs block [e][f][node] of a group as X[node][f*8 + e] (columns of
+// elements past the end get 0): loads first, then the barrier that frees X,
+// then the stores; `between` runs after the loads are issued
+template <int Nq, int Nf, int LD, int THREADS, typename F>
+__device__ __forceinline__ void stage_rhs(const double *__restrict__ rhs, int k0, int ne, double *X,
+                                          F between) {
+  constexpr int EW = 8, TOT = EW * Nf * Nq, IT = (TOT + THREADS - 1) / THREADS;
+  const double *src = rhs + (size_t)k0 * Nf * Nq;
+  const int lim = ne * Nf * Nq;
+  double v[IT];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int t = threadIdx.x + THREADS * it;
+    v[it] = t < lim ? src[t] : 0.0;
+  }
+  between();
+  __syncthreads();  // the previous group's last reads of X and Y are done
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int t = threadIdx.x + THREADS * it;
+    if (t < TOT) {
+      const int e = t / (Nf * Nq), rem = t - e * (Nf * Nq);
+      const int f = rem / Nq, n = rem - f * Nq;
+      X[n * LD + f * EW + e] = v[it];
+    }
+  }
+}
+
+template <int DIM, int N, bool CURVED>
+__global__ void __launch_bounds__(UpdMmaCfg<DIM, N, CURVED>::threads, UpdMmaCfg<DIM, N, CURVED>::min_ctas)
 update_mma_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
                   const double *__restrict__ VfPq, double fa, double fb, double fdt,
                   double *__restrict__ rhsQ, double *__restrict__ resQ, double *__restrict__ Q,
                   double *__restrict__ Qf, Phys P) {
   using C = UpdMmaCfg<DIM, N, CURVED>;
-  constexpr int Nq = C::Nq, NF = C::NF, Nf = C::Nf, EW = C::EW, KS = C::KS, KP = C::KP,
-                LD = C::LD, MQ = C::MQ, MO = C::MO, W = C::WARPS;
+  constexpr int Nq = C::Nq, Nf = C::Nf, EW = C::EW, KP = C::KP, LD = C::LD, MQ = C::MQ;
   extern __shared__ double smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *X = smem;
@@ -174,124 +315,14 @@ update_mma_kernel(int K, const double *__restrict__ Jq, const double *__restrict
   for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
     const int k0 = g * EW;
     const int ne = min(EW, K - k0);
-    bool ev[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) ev[i] = 2 * (lane & 3) + i < ne;
-
-    // ---- stage the group's rhs block [e][f][node] as X[node][f*8 + e]; the
-    // LSRK operands of this warp's first m-tile are loaded alongside
-    constexpr int TOT = EW * Nf * Nq, IT = (TOT + C::threads - 1) / C::threads;
+    // the LSRK operands of this warp's first m-tile load alongside the rhs block
     double res0[2][Nf], q0[2][Nf], Jv[2];
-    {
-      const double *src = rhsQ + (size_t)k0 * Nf * Nq;
-      const int lim = ne * Nf * Nq;
-      double v[IT];
-#pragma unroll
-      for (int it = 0; it < IT; ++it) {
-        const int t = threadIdx.x + C::threads * it;
-        v[it] = t < lim ? src[t] : 0.0;
-      }
+    stage_rhs<Nq, Nf, LD, C::threads>(rhsQ, k0, ne, X, [&] {
       if (warp < MQ) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, warp, lane, res0, q0, Jv);
-      __syncthreads();  // the previous group's last reads of X and Y are done
-#pragma unroll
-      for (int it = 0; it < IT; ++it) {
-        const int t = threadIdx.x + C::threads * it;
-        if (t < TOT) {
-          const int e = t / (Nf * Nq), rem = t - e * (Nf * Nq);
-          const int f = rem / Nq, n = rem - f * Nq;
-          X[n * LD + f * EW + e] = v[it];
-        }
-      }
-    }
+    });
     __syncthreads();
-
-    double a[KS], D[Nf][2];
-    // ---- r = M^{-1} rhs (affine: -2 VqPq rhs / J; WADG: VqPq(-2 VqPq rhs / J))
-    const double *R = X;  // the operand of the last product before the update
-    if (CURVED) {
-      for (int mt = warp; mt < MQ; mt += W) {
-        load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
-        mtile_gemm<KS, Nf, LD>(a, X, lane, D);
-        mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, -2.0, Jq, k0, ne);
-      }
-      __syncthreads();
-      R = Y;
-    }
-    // the update proper; V(U) goes to the other buffer (affine: Y; WADG: X,
-    // scaled by J for the projection that follows)
-    double *Vb = CURVED ? X : Y;
-    for (int mt = warp; mt < MQ; mt += W) {
-      if (mt != warp) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, mt, lane, res0, q0, Jv);
-      const int m = mt * 8 + (lane >> 2);
-      load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
-      mtile_gemm<KS, Nf, LD>(a, R, lane, D);
-      if (m < Nq) {
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int e = 2 * (lane & 3) + i;
-          const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
-          double U[Nf], V[Nf];
-#pragma unroll
-          for (int f = 0; f < Nf; ++f) {
-            const double r = CURVED ? D[f][i] : -2.0 * D[f][i] / Jv[i];
-            const double res = fa * res0[i][f] + fdt * r;
-            U[f] = q0[i][f] + fb * res;
-            if (ev[i]) {
-              resQ[id + f * Nq] = res;
-              Q[id + f * Nq] = U[f];
-            }
-          }
-          if (ev[i]) {
-            VU<DIM>(U, V, P);
-          } else {
-#pragma unroll
-            for (int f = 0; f < Nf; ++f) V[f] = 0.0;
-          }
-#pragma unroll
-          for (int f = 0; f < Nf; ++f) Vb[m * LD + f * EW + e] = CURVED ? V[f] * Jv[i] : V[f];
-        }
-      }
-    }
-    __syncthreads();
-    const double *Xo = Y;  // the operand of the output projection
-    if (CURVED) {
-      // v~ = VqPq((VqPq(v J)) / J): X -> Y -> X
-      for (int mt = warp; mt < MQ; mt += W) {
-        load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
-        mtile_gemm<KS, Nf, LD>(a, X, lane, D);
-        mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, 1.0, Jq, k0, ne);
-      }
-      __syncthreads();
-      for (int mt = warp; mt < MQ; mt += W) {
-        load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
-        mtile_gemm<KS, Nf, LD>(a, Y, lane, D);
-        mtile_store<Nq, Nf, LD, false>(X, mt, lane, D, 1.0, Jq, k0, ne);
-      }
-      __syncthreads();
-      Xo = X;
-    }
-
-    // ---- Qf = U(VfPq v), rhsQ = U(VqPq v)
-    for (int mt = warp; mt < MO; mt += W) {
-      load_afrag_out<KS, Nq, NF>(VfPq, VqPq, mt, lane, a);
-      mtile_gemm<KS, Nf, LD>(a, Xo, lane, D);
-      const int m = mt * 8 + (lane >> 2);
-      if (m >= NF + Nq) continue;
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        if (!ev[i]) continue;
-        const int e = 2 * (lane & 3) + i;
-        double V[Nf], U[Nf];
-#pragma unroll
-        for (int f = 0; f < Nf; ++f) V[f] = D[f][i];
-        UV<DIM>(V, U, P);
-        double *out = m < NF ? Qf + (size_t)(k0 + e) * NF * Nf + m
-                             : rhsQ + (size_t)(k0 + e) * Nq * Nf + (m - NF);
-        const int ld = m < NF ? NF : Nq;
-#pragma unroll
-        for (int f = 0; f < Nf; ++f) out[f * ld] = U[f];
-      }
-    }
+    update_group<DIM, N, CURVED>(k0, ne, warp, lane, X, Y, Jq, VqPq, VfPq, fa, fb, fdt, resQ, Q,
+                                 rhsQ, Qf, P, res0, q0, Jv);
   }
 }
 
