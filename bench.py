@@ -60,10 +60,12 @@ def dist_env():
     return RP.env()
 
 
-def build_workload():
+def build_workload(builder=None):
+    """Geometry (host builder by default; the reference arm keeps it), stage-0
+    state and time step of the workload."""
     from scratch_wadge_b200 import ic as IC
     from scratch_wadge_b200 import mesh as M
-    geo = M.build_geometry(M.periodic_cube(NHEX), N)
+    geo = (builder or M.build_geometry)(M.periodic_cube(NHEX), N)
     Q, rhsQ, Qf, resQ = IC.stage0(geo, IC.initial_state(geo, "taylor_green"))
     dt, _ = IC.time_step(geo, CFL, N, nsteps=E2E_STEPS, wave_speed=IC.max_wave_speed(Q))
     return geo, dict(Q=Q, rhsQ=rhsQ, Qf=Qf, resQ=resQ), dt
@@ -204,7 +206,26 @@ def run_ours(args):
     from scratch_wadge_b200 import roofline as RF
     B.build()
 
-    geo, st0, dt = build_workload()
+    # geometry on the GPU (wadg_geofacs / wadg_match_faces); the host builder
+    # is timed beside it for the setup comparison
+    from scratch_wadge_b200 import geometry_gpu as GG
+    from scratch_wadge_b200 import mesh as M
+    GG.build_geometry_gpu(M.periodic_cube(2), N)  # module and operator upload, outside the timing
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    geo, st0, dt = build_workload(GG.build_geometry_gpu)
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    GG.build_geometry_gpu(M.periodic_cube(NHEX), N)
+    t_gpu = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    M.build_geometry(M.periodic_cube(NHEX), N)
+    t_host = time.perf_counter() - t0
+    setup = {"geometry_gpu_s": t_gpu, "geometry_host_s": t_host, "workload_setup_s": t_setup,
+             "note": "geometric factors + neighbour maps of the workload mesh: the GPU builder "
+                     "(wadg_geofacs + wadg_match_faces, with the host nodal coordinates and the "
+                     "copies) against the numpy host builder; workload_setup_s adds the stage-0 "
+                     "state and time step"}
     ops = geo.ops
     K, Nq, NfqNf, Np = geo.K, ops.Nq, ops.NfqNf, ops.Np
     dofs = K * Np
@@ -331,7 +352,7 @@ def run_ours(args):
                          "vol_ms_per_candidate": {str(w): t for w, t in vol_cand.items()}},
             "stage_variant": {"used": "fused" if use_fused else "three_kernels",
                               "ms_per_step": variants},
-            "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks}
+            "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks, "setup": setup}
     if not args.no_ensemble:
         line["ensemble"] = run_ensemble_measurement()
     if not args.no_adjoint:
@@ -430,9 +451,10 @@ def run_ensemble_measurement(steps=5, warmup=2):
     per time step) against the plain one-instance-per-launch path, same dt and
     steps; throughput in DOF*stages/s, timed with CUDA events."""
     from scratch_wadge_b200 import ensemble as EN
+    from scratch_wadge_b200 import geometry_gpu as GG
     t0 = time.perf_counter()
     inst = EN.draw_instances(n=256, kmin=200, kmax=8192, degrees=(2, 3, 4), seed=0)
-    parts = [EN.build_instance(i) for i in inst]
+    parts = [EN.build_instance(i, builder=GG.build_geometry_gpu) for i in inst]
     dt = EN.common_dt(parts)
     setup_s = time.perf_counter() - t0
     out = {"instances": len(inst), "K_total": sum(i.K for i in inst),

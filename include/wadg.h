@@ -145,6 +145,54 @@ int wadg_euler_update_2d_curved(wadg_ctx *ctx, int K, const double *Jq,
                                 double fa, double fb, double fdt, double *rhsQ,
                                 double *resQ, double *Q, double *Qf);
 
+/* ------------------------------------------------------------ geometry
+ * GPU builder of the geometric data the kernels read -- the work the
+ * reference does on the host in host_operators_new_2D / _3D
+ * (operators_c.cpp:39, 205: build_geofacs_2D / _3D, operators.cpp:343-719)
+ * and in its neighbour maps with the periodic fix-up (operators.cpp:765-1025,
+ * euler.c:3004-3175).  Inputs are the per-element nodal coordinates (the
+ * reference maps each element's vertices to its nodes, operators.cpp:365-367,
+ * 488-493; a curved mesh displaces them) and reference-element operators.
+ * Every pointer in wadg_geo_ops and every array argument is device memory;
+ * operators are column-major; the struct itself is read on the host. */
+typedef struct {
+  int dim, N;
+  int Np, Nq, NfqNf; /* nodes; volume and face quadrature points */
+  int Np2;           /* 3D: nodes of the degree N+1 element (curl form) */
+  const double *Vq;  /* Nq x Np */
+  const double *Vfq; /* NfqNf x Np */
+  const double *VqDr, *VqDs, *VqDt; /* Nq x Np: Vq Dr, Vq Ds, Vq Dt */
+  const double *VfDr, *VfDs, *VfDt; /* NfqNf x Np: Vfq Dr, ... */
+  const double *VqPq;               /* Nq x Nq */
+  const double *nrJ, *nsJ, *ntJ;    /* NfqNf reference normals (scaled) */
+  const double *V12;                /* Np2 x Np: degree N -> N+1 nodes (3D) */
+  const double *Dr2, *Ds2, *Dt2;    /* Np2 x Np2 derivatives at degree N+1 */
+  const double *V21;                /* Np x Np2: degree N+1 -> N nodes */
+} wadg_geo_ops;
+
+/* x: nodal coordinates [K][dim][Np].  Out: vgeo [K][Nvgeo][Nq],
+ * vfgeo [K][Nvgeo][NfqNf], fgeo [K][Nfgeo][NfqNf], Jq [K][Nq] (= VqPq J),
+ * xyzq [K][3][Nq], xyzf [K][3][NfqNf] (2D: third row 0).  2D: the
+ * cross-product form (operators.cpp:385-440); 3D: J and sJ from the
+ * cross-product form, the metric terms from Kopriva's curl form at degree
+ * N+1 (operators.cpp:542-719), so curved meshes keep the discrete GCL.
+ * stream: a cudaStream_t (NULL: the legacy default stream). */
+int wadg_geofacs(const wadg_geo_ops *ops, int K, const double *x, double *vgeo,
+                 double *vfgeo, double *fgeo, double *Jq, double *xyzq,
+                 double *xyzf, void *stream);
+/* mapPq [K][NfqNf] of a mesh periodic in every direction of the box
+ * [lo, hi] (host arrays of dim doubles): the neighbour face point of every
+ * face quadrature point by physical coincidence, field-strided
+ * (j + e NfqNf Nfields, euler.c:3156-3174).  xa: the nodal coordinates
+ * that define the topology (a curved mesh's undisplaced ones) [K][dim][Np];
+ * only ops->dim, Np, NfqNf and Vfq are read.  work: device scratch of
+ * wadg_match_faces_workspace(K, NfqNf) bytes.  Synchronises the stream;
+ * WADG_ERR_INVALID when the face points do not pair up across elements. */
+size_t wadg_match_faces_workspace(int K, int NfqNf);
+int wadg_match_faces(const wadg_geo_ops *ops, int K, const double *xa,
+                     const double *lo, const double *hi, void *work,
+                     size_t work_bytes, uint32_t *mapPq, void *stream);
+
 /* ------------------------------------------------------------ diagnostics
  * euler_3d_compute_aux: Euler3D.okl:3888 -- aux[k] = sum_i 1/2 |m|^2/rho J w,
  * the kinetic energy of element k (the reference sums aux on the host; its

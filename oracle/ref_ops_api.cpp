@@ -12,6 +12,11 @@
  *   wadgref_ops_new / wadgref_ops_free
  *       host_operators_new_2D / _3D on a caller-supplied mesh
  *       (operators_c.cpp:39, 205): geometric factors, Jq, maps.
+ *   wadgref_geofacs
+ *       the geometric factors, Jq and physical node coordinates that
+ *       host_operators_new_2D / _3D build for a mesh given by its element
+ *       vertex coordinates (build_geofacs_2D / _3D, operators.cpp:343-719),
+ *       copied out in the layouts the kernels read.
  */
 #include "operators.h"
 #include "operators_c.h"
@@ -141,6 +146,47 @@ void wadgref_ops_free(host_operators_t *ops)
     free(ops->Drstq);
   host_operators_free(ops);
   free(ops);
+}
+
+/* EToVX: E columns of the element's vertex coordinates, vertex-major
+ * (x0 y0 [z0] x1 y1 [z1] ...), as euler.c passes them.  Connectivity is
+ * set to "every face its own neighbour": the maps are not copied out.
+ * Outputs: vgeo [E][Nvgeo][Nq], vfgeo [E][Nvgeo][NfqNf],
+ * fgeo [E][Nfgeo][NfqNf], Jq [E][Nq], xyzq [E][3][Nq] and
+ * xyzf [E][3][NfqNf] (2D: the third row is left as allocated). */
+int wadgref_geofacs(int dim, int N, int M, uint32_t E, double *EToVX, double *vgeo,
+                    double *vfgeo, double *fgeo, double *Jq, double *xyzq, double *xyzf)
+{
+  const int nf = dim + 1;
+  uint32_t *EToE = new uint32_t[(size_t)nf * E];
+  uint8_t *EToF = new uint8_t[(size_t)nf * E];
+  uint8_t *EToO = new uint8_t[(size_t)nf * E];
+  for (uint32_t e = 0; e < E; ++e)
+    for (int f = 0; f < nf; ++f)
+    {
+      EToE[f + nf * e] = e;
+      EToF[f + nf * e] = (uint8_t)f;
+      EToO[f + nf * e] = 0;
+    }
+  host_operators_t *ops = wadgref_ops_new(dim, N, M, E, EToE, EToF, EToO, EToVX);
+  delete[] EToE;
+  delete[] EToF;
+  delete[] EToO;
+  if (!ops)
+    return 1;
+  const size_t Nq = ops->Nq, NF = (size_t)ops->Nfq * ops->Nfaces;
+  std::memcpy(vgeo, ops->vgeo, sizeof(double) * Nq * ops->Nvgeo * E);
+  std::memcpy(vfgeo, ops->vfgeo, sizeof(double) * NF * ops->Nvgeo * E);
+  std::memcpy(fgeo, ops->fgeo, sizeof(double) * NF * ops->Nfgeo * E);
+  std::memcpy(Jq, ops->Jq, sizeof(double) * Nq * E);
+  for (uint32_t e = 0; e < E; ++e)
+    for (int d = 0; d < dim; ++d)
+    {
+      std::memcpy(xyzq + (e * 3 + d) * Nq, ops->xyzq + (e * 3 + d) * Nq, sizeof(double) * Nq);
+      std::memcpy(xyzf + (e * 3 + d) * NF, ops->xyzf + (e * 3 + d) * NF, sizeof(double) * NF);
+    }
+  wadgref_ops_free(ops);
+  return 0;
 }
 
 } /* extern "C" */

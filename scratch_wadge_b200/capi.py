@@ -107,6 +107,10 @@ def lib():
         L.wadg_adjoint_reverse.argtypes = [v, v, v]
         L.wadg_adjoint_rhs.argtypes = [v, v, v]
         L.wadg_adjoint_rhs_vjp.argtypes = [v, v, v, v]
+        L.wadg_geofacs.argtypes = [v, i] + [v] * 8
+        L.wadg_match_faces_workspace.argtypes = [i, i]
+        L.wadg_match_faces_workspace.restype = ctypes.c_size_t
+        L.wadg_match_faces.argtypes = [v, i, v, v, v, v, ctypes.c_size_t, v, v]
         _lib = L
     return _lib
 

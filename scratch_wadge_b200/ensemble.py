@@ -58,8 +58,10 @@ def draw_instances(n=256, kmin=200, kmax=8192, degrees=(2, 3, 4), seed=0):
     return out
 
 
-def build_instance(inst: Instance, gamma=1.4):
-    geo = M.build_geometry(M.periodic_square(inst.nx, inst.ny), inst.N)
+def build_instance(inst: Instance, gamma=1.4, builder=None):
+    """Geometry (builder(mesh, N): mesh.build_geometry by default, or
+    geometry_gpu.build_geometry_gpu) and stage-0 state of one instance."""
+    geo = (builder or M.build_geometry)(M.periodic_square(inst.nx, inst.ny), inst.N)
     U0 = IC.initial_state(geo, "vortex", gamma, beta=inst.beta, x0=inst.x0, y0=inst.y0)
     Q, rhsQ, Qf, resQ = IC.stage0(geo, U0, gamma)
     return geo, dict(Q=Q, rhsQ=rhsQ, Qf=Qf, resQ=resQ)
