@@ -22,7 +22,10 @@ def rel(a, b):
 
 
 def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """The stage fixtures (gen_golden.py); the geometry fixtures geo*.npz
+    (gen_geometry.py) are read by tests/test_geometry.py."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not os.path.basename(p).startswith("geo"))
 
 
 class Case:
