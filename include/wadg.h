@@ -205,6 +205,17 @@ int wadg_euler_3d_compute_aux(wadg_ctx *ctx, int K, const double *Jq,
                               const double *wq, const double *Q, double *aux);
 int wadg_element_entropy(wadg_ctx *ctx, int K, const double *Jq,
                          const double *wq, const double *Q, double *S);
+/* The entropy balance of the RHS, per element: out[k] = sum_i wq_i v~_i .
+ * rhs_i, with rhs [K][Nf][Nq] the RHS after the volume and surface kernels
+ * (before the inverse mass) and v~ the projected entropy variables of the
+ * state Q the stage started from (affine: VqPq V(Q); curved:
+ * VqPq((VqPq(V(Q) J))/J), J = Jq, which only curved reads).  Summed over a
+ * periodic mesh: 0 to round-off without the surface penalty (tau = 0),
+ * positive with it.  The device-side form of the entropy checks the
+ * reference runs on the host (euler.c:4135-4156). */
+int wadg_entropy_rhs(wadg_ctx *ctx, int K, int curved, const double *wq,
+                     const double *Jq, const double *VqPq, const double *Q,
+                     const double *rhs, double *out);
 
 /* ------------------------------------------------------------ fused stage
  * One LSRK stage -- vol, surf and update of the kernels above -- in a single

@@ -96,6 +96,7 @@ def lib():
         L.wadg_ctx_set_stream.argtypes = [v, v]
         L.wadg_euler_3d_compute_aux.argtypes = [v, i, v, v, v, v]
         L.wadg_element_entropy.argtypes = [v, i, v, v, v, v]
+        L.wadg_entropy_rhs.argtypes = [v, i, i] + [v] * 6
         L.wadg_vol_warps_candidates.argtypes = [v, i, ctypes.POINTER(ctypes.c_int)]
         L.wadg_ctx_set_vol_warps.argtypes = [v, i, i]
         L.wadg_ctx_get_vol_warps.argtypes = [v]
@@ -177,6 +178,11 @@ class Context:
     def compute_aux(self, K, Jq, wq, Q, aux):
         """per-element kinetic energy (euler_3d_compute_aux)"""
         check(lib().wadg_euler_3d_compute_aux(self.h, K, Jq, wq, Q, aux), "compute_aux")
+
+    def entropy_rhs(self, curved, K, wq, Jq, VqPq, Q, rhs, out):
+        """per-element entropy balance sum_i w v~ . rhs (wadg_entropy_rhs)"""
+        check(lib().wadg_entropy_rhs(self.h, K, int(curved), wq, Jq, VqPq, Q, rhs, out),
+              "entropy_rhs")
 
     def element_entropy(self, K, Jq, wq, Q, S):
         """per-element entropy integral sum_i w J (-rho s)"""

@@ -296,6 +296,14 @@ int launch_integral(const wadg_ctx *c, int K, const double *Jq, const double *wq
   return after_launch("element integral kernel");
 }
 
+template <int DIM, int N, bool CURVED>
+int launch_entropy_rhs(const wadg_ctx *c, int K, const double *wq, const double *Jq,
+                       const double *VqPq, const double *Q, const double *rhs, double *out) {
+  entropy_rhs_kernel<DIM, N, CURVED><<<(K + 7) / 8, 256, 0, c->stream>>>(K, wq, Jq, VqPq, Q, rhs,
+                                                                         out, c->phys);
+  return after_launch("entropy RHS kernel");
+}
+
 extern "C" {
 
 const char *wadg_last_error(void) { return g_err.c_str(); }
@@ -399,6 +407,19 @@ int wadg_element_entropy(wadg_ctx *c, int K, const double *Jq, const double *wq,
   if (K == 0) return WADG_OK;
   if (any_null({Jq, wq, Q, S})) return fail(WADG_ERR_INVALID, "null pointer argument");
   WADG_DISPATCH(c, return (launch_integral<D_, N_, true>(c, K, Jq, wq, Q, S)));
+}
+
+int wadg_entropy_rhs(wadg_ctx *c, int K, int curved, const double *wq, const double *Jq,
+                     const double *VqPq, const double *Q, const double *rhs, double *out) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  if (K < 0) return fail(WADG_ERR_INVALID, "K < 0");
+  if (K == 0) return WADG_OK;
+  if (any_null({wq, VqPq, Q, rhs, out}) || (curved && !Jq))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  if (curved) {
+    WADG_DISPATCH(c, return (launch_entropy_rhs<D_, N_, true>(c, K, wq, Jq, VqPq, Q, rhs, out)));
+  }
+  WADG_DISPATCH(c, return (launch_entropy_rhs<D_, N_, false>(c, K, wq, Jq, VqPq, Q, rhs, out)));
 }
 
 // ------------------------------------------------------------------ 3D
