@@ -185,13 +185,43 @@ int wadg_geofacs(const wadg_geo_ops *ops, int K, const double *x, double *vgeo,
  * face quadrature point by physical coincidence, field-strided
  * (j + e NfqNf Nfields, euler.c:3156-3174).  xa: the nodal coordinates
  * that define the topology (a curved mesh's undisplaced ones) [K][dim][Np];
- * only ops->dim, Np, NfqNf and Vfq are read.  work: device scratch of
- * wadg_match_faces_workspace(K, NfqNf) bytes.  Synchronises the stream;
- * WADG_ERR_INVALID when the face points do not pair up across elements. */
+ * only ops->dim, Np, NfqNf and Vfq are read.  unpaired_self != 0: a face
+ * point with no partner is a boundary point and its own neighbour
+ * (mapPq(j) = j, the reference's idM == idP); 0: an error.  work: device
+ * scratch of wadg_match_faces_workspace(K, NfqNf) bytes.  Synchronises the
+ * stream; WADG_ERR_INVALID when the face points do not pair up across
+ * elements. */
 size_t wadg_match_faces_workspace(int K, int NfqNf);
 int wadg_match_faces(const wadg_geo_ops *ops, int K, const double *xa,
-                     const double *lo, const double *hi, void *work,
-                     size_t work_bytes, uint32_t *mapPq, void *stream);
+                     const double *lo, const double *hi, int unpaired_self,
+                     void *work, size_t work_bytes, uint32_t *mapPq,
+                     void *stream);
+
+/* ------------------------------------------------------------ mesh I/O
+ * The host driver's mesh files.  wadg_mesh_read_gmsh reads ASCII gmsh 2.x as
+ * host_mesh_read_msh does (euler.c:556-833): the nodes; the elements of type
+ * 2 (dim 2, triangles) or 4 (dim 3, tetrahedra), others and all tags
+ * skipped; $Periodic skipped.  Negatively oriented elements get vertices 1
+ * and 2 swapped (counted in `flipped`).  The periodic box lo/hi is the
+ * bounding box of the elements' vertices, the box modify_mapP matches
+ * periodic faces on (euler.c:3013-3050).  wadg_mesh_write_mfem writes
+ * "MFEM mesh v1.0" as host_mesh_write_mfem does (euler.c:1771-1857):
+ * per-element vertex copies EToVX [K][dim+1][dim] and the faces flagged in
+ * bface [K][dim+1] (faces whose points are their own neighbours) as
+ * boundary elements.  wadg_mesh_write_gmsh writes ASCII gmsh 2.2 (VX
+ * [Nv][dim], EToV [K][dim+1] 0-based) for the reference to read.  All host
+ * memory; no CUDA call. */
+typedef struct wadg_mesh wadg_mesh;
+int wadg_mesh_read_gmsh(const char *path, int dim, wadg_mesh **out);
+int wadg_mesh_sizes(const wadg_mesh *m, int *dim, int64_t *Nv, int64_t *K,
+                    int64_t *flipped);
+int wadg_mesh_get(const wadg_mesh *m, double *VX, int64_t *EToV, double *lo,
+                  double *hi);
+void wadg_mesh_destroy(wadg_mesh *m);
+int wadg_mesh_write_gmsh(const char *path, int dim, int64_t Nv,
+                         const double *VX, int64_t K, const int64_t *EToV);
+int wadg_mesh_write_mfem(const char *path, int dim, int64_t K,
+                         const double *EToVX, const uint8_t *bface);
 
 /* ------------------------------------------------------------ diagnostics
  * euler_3d_compute_aux: Euler3D.okl:3888 -- aux[k] = sum_i 1/2 |m|^2/rho J w,

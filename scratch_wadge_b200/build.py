@@ -14,7 +14,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")) +
+                  glob.glob(os.path.join(HERE, "csrc", "*.cpp")))
 
 
 def deps():

@@ -111,7 +111,16 @@ def lib():
         L.wadg_geofacs.argtypes = [v, i] + [v] * 8
         L.wadg_match_faces_workspace.argtypes = [i, i]
         L.wadg_match_faces_workspace.restype = ctypes.c_size_t
-        L.wadg_match_faces.argtypes = [v, i, v, v, v, v, ctypes.c_size_t, v, v]
+        L.wadg_match_faces.argtypes = [v, i, v, v, v, i, v, ctypes.c_size_t, v, v]
+        i64 = ctypes.c_int64
+        L.wadg_mesh_read_gmsh.argtypes = [ctypes.c_char_p, i, ctypes.POINTER(ctypes.c_void_p)]
+        L.wadg_mesh_sizes.argtypes = [v, ctypes.POINTER(i), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                      ctypes.POINTER(i64)]
+        L.wadg_mesh_get.argtypes = [v] * 5
+        L.wadg_mesh_destroy.argtypes = [v]
+        L.wadg_mesh_destroy.restype = None
+        L.wadg_mesh_write_gmsh.argtypes = [ctypes.c_char_p, i, i64, v, i64, v]
+        L.wadg_mesh_write_mfem.argtypes = [ctypes.c_char_p, i, i64, v, v]
         _lib = L
     return _lib
 

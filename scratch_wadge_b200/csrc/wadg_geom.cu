@@ -19,9 +19,10 @@
 // every direction, by physical coincidence: each point's position in the
 // periodic box is quantised to 2^-21 of the box per coordinate, the quantised
 // positions go into an open-addressing hash table (bounded linear probing,
-// atomicCAS on the key), and every key must hold exactly two points of two
-// different elements.  Anything else is reported as an error, as the host
-// builder does.
+// atomicCAS on the key), and every key must hold two points of two different
+// elements, or, where the caller allows boundaries, one point, which becomes
+// its own neighbour (the reference's idM == idP boundary points).  Anything
+// else is reported as an error, as the host builder does.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -307,13 +308,17 @@ __global__ void insert_kernel(int n, const unsigned long long *__restrict__ keys
   atomicOr(flag, 2);  // table full (cannot happen at load 1/2)
 }
 
-__global__ void pair_kernel(unsigned tsize, const unsigned *__restrict__ tcnt,
+__global__ void pair_kernel(unsigned tsize, int unpaired_self, const unsigned *__restrict__ tcnt,
                             const unsigned *__restrict__ ta, const unsigned *__restrict__ tb,
                             unsigned *partner, int *flag) {
   const unsigned h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= tsize) return;
   const unsigned c = tcnt[h];
   if (c == 0) return;
+  if (c == 1 && unpaired_self) {  // a boundary point: its own neighbour
+    partner[ta[h]] = ta[h];
+    return;
+  }
   if (c != 2) {
     atomicOr(flag, 1);
     return;
@@ -327,7 +332,7 @@ __global__ void mapPq_kernel(int n, int NF, int Nfields, const unsigned *__restr
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const unsigned q = partner[p];
-  if (q == 0xffffffffu || (int)(q / NF) == p / NF) {
+  if (q == 0xffffffffu || ((int)(q / NF) == p / NF && (int)q != p)) {
     atomicOr(flag, 4);
     mapPq[p] = (uint32_t)p;
     return;
@@ -415,8 +420,8 @@ size_t wadg_match_faces_workspace(int K, int NfqNf) {
 }
 
 int wadg_match_faces(const wadg_geo_ops *ops, int K, const double *xa, const double *lo,
-                     const double *hi, void *work, size_t work_bytes, uint32_t *mapPq,
-                     void *stream) {
+                     const double *hi, int unpaired_self, void *work, size_t work_bytes,
+                     uint32_t *mapPq, void *stream) {
   if (!ops || (ops->dim != 2 && ops->dim != 3) || !ops->Vfq || ops->Np <= 0 || ops->NfqNf <= 0)
     return gfail(WADG_ERR_INVALID, "wadg_match_faces: incomplete operator set");
   if (K < 0) return gfail(WADG_ERR_INVALID, "wadg_match_faces: K < 0");
@@ -445,7 +450,8 @@ int wadg_match_faces(const wadg_geo_ops *ops, int K, const double *xa, const dou
   face_keys_kernel<<<K, 64, sizeof(double) * dim * Np, s>>>(dim, Np, NF, ops->Vfq, xa, box, w.keys);
   insert_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, w.keys, w.tkey, w.tcnt, w.ta, w.tb,
                                                  w.tsize - 1, w.flag);
-  pair_kernel<<<(w.tsize + 255) / 256, 256, 0, s>>>(w.tsize, w.tcnt, w.ta, w.tb, w.partner, w.flag);
+  pair_kernel<<<(w.tsize + 255) / 256, 256, 0, s>>>(w.tsize, unpaired_self, w.tcnt, w.ta, w.tb,
+                                                     w.partner, w.flag);
   mapPq_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, NF, dim + 2, w.partner, mapPq, w.flag);
   if ((e = cudaGetLastError()) != cudaSuccess) return gfail(WADG_ERR_CUDA, "wadg_match_faces: launch", e);
   int flag = 0;

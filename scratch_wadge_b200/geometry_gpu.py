@@ -99,7 +99,8 @@ def build_geometry_gpu(mesh: M.Mesh, N: int) -> M.Geometry:
     hi = (ctypes.c_double * dim)(*mesh.hi)
     capi.check(L.wadg_match_faces(ctypes.byref(dops.struct), K,
                                   (xad if xad is not None else xd).data_ptr(), lo, hi,
-                                  work.data_ptr(), nbytes, mapPq.data_ptr(), stream), "match_faces")
+                                  int(mesh.boundary_self), work.data_ptr(), nbytes,
+                                  mapPq.data_ptr(), stream), "match_faces")
     h = {k: v.cpu().numpy() for k, v in out.items()}
     if np.any(h["Jq"] <= 0):
         raise ValueError("mesh has elements with non-positive Jacobian")

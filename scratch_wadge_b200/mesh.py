@@ -38,6 +38,7 @@ class Mesh:
     lo: np.ndarray            # domain lower corner (dim,)
     hi: np.ndarray            # domain upper corner (dim,)
     warp: object = None       # optional callable (x,y[,z]) -> displaced coords
+    boundary_self: bool = False  # unpaired face points are boundary points (mapPq(j) = j)
 
     @property
     def K(self):
@@ -142,7 +143,7 @@ def build_geometry(mesh: Mesh, N: int) -> Geometry:
     xq = np.stack([ops.Vq @ x[d] for d in range(mesh.dim)], axis=0)             # (dim,Nq,K)
     xf = np.stack([ops.Vfq @ x[d] for d in range(mesh.dim)], axis=0)
     xfa = np.stack([ops.Vfq @ xa[d] for d in range(mesh.dim)], axis=0)
-    mapPq = _match_faces(mesh, ops, xfa)
+    mapPq = _match_faces(mesh, ops, xfa, mesh.boundary_self)
     pad = lambda a: np.concatenate([a, np.zeros((3 - mesh.dim,) + a.shape[1:])], 0)
     xyzq = np.ascontiguousarray(pad(xq).transpose(2, 0, 1))
     xyzf = np.ascontiguousarray(pad(xf).transpose(2, 0, 1))
@@ -230,13 +231,16 @@ def _geofacs_3d(ops, x):
     return {"vq": Gq, "vf": Gf, "fg": [nxJ, nyJ, nzJ, sJ], "J": J}
 
 
-def _match_faces(mesh: Mesh, ops, xf) -> np.ndarray:
+def _match_faces(mesh: Mesh, ops, xf, unpaired_self=False) -> np.ndarray:
     """Neighbour of every face quadrature point, periodic in every direction,
     by matching physical coordinates (the result the reference reaches with
-    build_maps_2D/3D plus modify_mapP).  Returns field-strided mapPq."""
+    build_maps_2D/3D plus modify_mapP).  With unpaired_self, a point with no
+    partner is a boundary point and its own neighbour (the reference's
+    idM == idP); otherwise it is an error.  Returns field-strided mapPq."""
     dim, K, NfqNf = mesh.dim, mesh.K, ops.NfqNf
     L = mesh.hi - mesh.lo
-    pts = xf.transpose(2, 1, 0).reshape(K * NfqNf, dim)  # point id = j + e*NfqNf
+    n = K * NfqNf
+    pts = xf.transpose(2, 1, 0).reshape(n, dim)  # point id = j + e*NfqNf
     t = (pts - mesh.lo) / L
     t = t - np.floor(t)
     t[t > 1 - 1e-9] = 0.0
@@ -244,16 +248,21 @@ def _match_faces(mesh: Mesh, ops, xf) -> np.ndarray:
     key = np.round(t / h).astype(np.int64)
     order = np.lexsort(key.T[::-1])
     ks = key[order]
-    same_next = np.all(ks[1:] == ks[:-1], axis=1)
-    if not (np.all(same_next[0::2]) and not np.any(same_next[1::2])):
+    start = np.ones(n, dtype=bool)
+    start[1:] = np.any(ks[1:] != ks[:-1], axis=1)
+    first = np.flatnonzero(start)
+    size = np.diff(np.append(first, n))
+    if np.any(size > 2) or (not unpaired_self and np.any(size == 1)):
         raise ValueError("face points do not pair up: mesh is not a closed periodic mesh")
-    a, b = order[0::2], order[1::2]
-    partner = np.empty(K * NfqNf, dtype=np.int64)
+    partner = np.arange(n, dtype=np.int64)
+    two = first[size == 2]
+    a, b = order[two], order[two + 1]
     partner[a] = b
     partner[b] = a
     e = partner // NfqNf
     j = partner % NfqNf
-    if np.any(e == np.arange(K * NfqNf) // NfqNf):
+    own = np.arange(n) // NfqNf
+    if np.any((e == own) & (partner != np.arange(n))):
         raise ValueError("face point matched inside its own element")
     mapPq = (j + e * NfqNf * ops.Nfields).astype(np.uint32)
     return mapPq.reshape(K, NfqNf)

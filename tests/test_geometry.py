@@ -68,5 +68,5 @@ def test_geometry_abi_validation():
     assert L.wadg_match_faces_workspace(100, 12) >= 100 * 12 * 8
     lo = (ctypes.c_double * 2)(0.0, 0.0)
     hi = (ctypes.c_double * 2)(1.0, 1.0)
-    assert L.wadg_match_faces(ctypes.byref(ops), 0, None, lo, hi, None, 0, None, None) == 0
-    assert L.wadg_match_faces(ctypes.byref(ops), 4, None, lo, hi, None, 0, None, None) != 0
+    assert L.wadg_match_faces(ctypes.byref(ops), 0, None, lo, hi, 0, None, 0, None, None) == 0
+    assert L.wadg_match_faces(ctypes.byref(ops), 4, None, lo, hi, 0, None, 0, None, None) != 0

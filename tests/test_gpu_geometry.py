@@ -80,3 +80,22 @@ def test_match_faces_rejects_a_non_periodic_box(cuda):
     bad = M.Mesh(2, mesh.VX, mesh.EToV, mesh.lo, mesh.hi + np.array([20.0, 0.0]))
     with pytest.raises(capi.WadgError):
         GG.build_geometry_gpu(bad, 3)
+
+
+def test_gpu_builder_on_gmsh_meshes(cuda, tmp_path):
+    """Meshes through the gmsh reader: an unstructured-looking periodic mesh,
+    and a mesh inside a larger box whose outer face points become their own
+    neighbours (the reference's boundary semantics)."""
+    from scratch_wadge_b200 import meshio as IO
+    from tests.test_meshio import jittered_square
+    p = str(tmp_path / "j.msh")
+    IO.write_gmsh(jittered_square(8), p)
+    m = IO.read_gmsh(p, 2)
+    for mesh in (m, M.Mesh(2, m.VX, m.EToV, m.lo - 1.0, m.hi + 1.0, boundary_self=True)):
+        for N in (2, 4):
+            h = M.build_geometry(mesh, N)
+            g = GG.build_geometry_gpu(mesh, N)
+            assert np.array_equal(g.mapPq, h.mapPq)
+            for k in FIELDS:
+                assert rel(getattr(g, k), getattr(h, k)) < RTOL, k
+    assert IO.boundary_faces(g).sum() > 0
