@@ -13,6 +13,7 @@
 #include "../../include/wadg.h"
 #include "wadg_diag.cuh"
 #include "wadg_kernels.cuh"
+#include "wadg_surf_mma.cuh"
 #include "wadg_update_mma.cuh"
 #include "wadg_vol.cuh"
 
@@ -49,12 +50,6 @@ int after_launch(const char *name) { return cuda_check(cudaGetLastError(), name)
 constexpr int pickE(int target, int per) { return per >= target ? 1 : target / per; }
 
 template <int DIM, int N> constexpr int volE() { return pickE(320, Elem<DIM, N>::NN); }
-// surface: small CTAs (2 elements at N=3) with ~64 registers per thread
-// (WADG_SURF_OCC in wadg_kernels.cuh) -- the fastest of a sweep of CTA size x
-// register cap on the 3D N=3 workload (0.072 ms vs 0.088 ms at 5 elements)
-template <int DIM, int N> constexpr int surfE() {
-  return pickE(128, Elem<DIM, N>::NfqNf > Elem<DIM, N>::Nq ? Elem<DIM, N>::NfqNf : Elem<DIM, N>::Nq);
-}
 
 template <int DIM, int N, bool CURVED>
 int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
@@ -180,11 +175,9 @@ int launch_stage(const wadg_ctx *c, int K, const double *vgeo, const double *vfg
 template <int DIM, int N>
 int launch_surf(const wadg_ctx *c, int K, const double *fgeo, const uint32_t *mapPq,
                 const double *VqLq, const double *Qf, const double *rhsQf, double *rhsQ) {
-  constexpr int E = surfE<DIM, N>();
-  using C = SurfCfg<DIM, N, E>;
-  const int grid = (K + E - 1) / E;
-  surf_kernel<DIM, N, E><<<grid, C::threads, C::smem, c->stream>>>(K, fgeo, mapPq, VqLq, Qf,
-                                                                    rhsQf, rhsQ, c->phys);
+  using C = SurfMmaCfg<DIM, N>;
+  surf_mma_kernel<DIM, N><<<(K + C::EW - 1) / C::EW, C::threads, C::smem, c->stream>>>(
+      K, fgeo, mapPq, VqLq, Qf, rhsQf, rhsQ, c->phys);
   return after_launch("surf kernel");
 }
 

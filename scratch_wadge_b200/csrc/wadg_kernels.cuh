@@ -1,5 +1,5 @@
-// The row-per-thread volume kernel and the surface kernel of one LSRK stage (the
-// update kernel is in wadg_update_mma.cuh), templated on
+// The row-per-thread volume kernel of one LSRK stage (the surface and update
+// kernels are in wadg_surf_mma.cuh and wadg_update_mma.cuh), templated on
 // dimension and degree.  One CTA handles E consecutive elements; everything an
 // element reads more than once is staged in shared memory.
 #pragma once
@@ -163,85 +163,6 @@ vol_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vf
     double *out = rhsQf + (size_t)k * NfqNf * Nf + i;
 #pragma unroll
     for (int f = 0; f < Nf; ++f) out[f * NfqNf] = acc[f];
-  }
-}
-
-// ---------------------------------------------------------------- surface
-// sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam-,lam+) sJ (u+ - u-),
-// rhsQ += VqLq sfS   (Euler3D.okl:3242-3473, Euler2D.okl:1357-1495)
-template <int DIM, int N, int E>
-struct SurfCfg {
-  using El = Elem<DIM, N>;
-  static constexpr int threads = E * (El::NfqNf > El::Nq ? El::NfqNf : El::Nq);
-  static constexpr size_t smem = sizeof(double) * E * El::Nfields * El::NfqNf;
-};
-
-// register cap from the launch bounds: about 1000 threads per SM (~64
-// registers each), enough warps to hide the neighbour-trace gathers
-template <int DIM, int N, int E>
-__global__ void __launch_bounds__(SurfCfg<DIM, N, E>::threads, 1024 / SurfCfg<DIM, N, E>::threads)
-surf_kernel(int K, const double *__restrict__ fgeo, const uint32_t *__restrict__ mapPq,
-            const double *__restrict__ VqLq, const double *__restrict__ Qf,
-            const double *__restrict__ rhsQf, double *__restrict__ rhsQ, Phys P) {
-  using El = Elem<DIM, N>;
-  constexpr int Nq = El::Nq, NfqNf = El::NfqNf, Nf = El::Nfields, NFG = El::Nfgeo;
-  extern __shared__ double smem[];
-  double (*sf)[Nf][NfqNf] = reinterpret_cast<double (*)[Nf][NfqNf]>(smem);
-  const int k0 = blockIdx.x * E;
-
-  for (int t = threadIdx.x; t < E * NfqNf; t += blockDim.x) {
-    const int e = t / NfqNf, i = t % NfqNf, k = k0 + e;
-    if (k >= K) continue;
-    const size_t idM = i + (size_t)k * NfqNf * Nf;
-    const size_t idP = mapPq[i + (size_t)k * NfqNf];
-    const double *fg = fgeo + (size_t)k * NfqNf * NFG + i;
-    double nJ[DIM];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) nJ[d] = fg[d * NfqNf];
-    const double sJ = fg[DIM * NfqNf];
-    double UM[Nf], UP[Nf];
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) {
-      UM[f] = Qf[idM + f * NfqNf];
-      UP[f] = Qf[idP + f * NfqNf];
-    }
-    const NodeState<DIM> M = node_state_nolog<DIM>(UM, 1, P);
-    const NodeState<DIM> Pp = node_state_nolog<DIM>(UP, 1, P);
-    double F[Nf];
-    ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
-    // wave speeds |u| + sqrt(gamma p / rho), p = rho / (2 beta)
-    double kM = 0.0, kP = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      kM = fma(M.vel[d], M.vel[d], kM);
-      kP = fma(Pp.vel[d], Pp.vel[d], kP);
-    }
-    const double pM = P.gm1 * (UM[Nf - 1] - 0.5 * M.rho * kM);
-    const double pP = P.gm1 * (UP[Nf - 1] - 0.5 * Pp.rho * kP);
-    const double lamM = sqrt(kM) + sqrt(P.gamma * pM / M.rho);
-    const double lamP = sqrt(kP) + sqrt(P.gamma * pP / Pp.rho);
-    const double tau = (DIM == 3) ? P.tau : 1.0;
-    const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
-    const double *rf = rhsQf + idM;
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) sf[e][f][i] = 0.5 * F[f] + rf[f * NfqNf] - Lfc * (UP[f] - UM[f]);
-  }
-  __syncthreads();
-
-  for (int t = threadIdx.x; t < E * Nq; t += blockDim.x) {
-    const int e = t / Nq, i = t % Nq, k = k0 + e;
-    if (k >= K) continue;
-    double val[Nf];
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) val[f] = 0.0;
-    for (int j = 0; j < NfqNf; ++j) {
-      const double w = __ldg(VqLq + i + j * Nq);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) val[f] = fma(w, sf[e][f][j], val[f]);
-    }
-    double *out = rhsQ + (size_t)k * Nq * Nf + i;
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) out[f * Nq] += val[f];
   }
 }
 
