@@ -23,6 +23,7 @@
 
 #include "../../include/wadg.h"
 #include "wadg_adjoint_kernels.cuh"
+#include "wadg_adjoint_mma.cuh"
 #include "wadg_app_impl.h"
 
 namespace wadg_internal {
@@ -104,14 +105,13 @@ int set_smem(F kern, size_t bytes, bool &done, const char *what) {
 template <int DIM, int N, bool CURVED>
 int launch_seed(const wadg_adjoint *j, cudaStream_t s, double b, double dt) {
   const wadg_app *a = j->app;
-  constexpr int E = pickE(256, Elem<DIM, N>::Nq);
-  using C = AdjSeedCfg<DIM, N, E>;
-  auto kern = adj_seed_kernel<DIM, N, CURVED, E>;
+  using C = AdjMmaCfg<DIM, N, CURVED>;
+  auto kern = adj_seed_mma_kernel<DIM, N, CURVED>;
   static bool attr = false;
   if (int r = set_smem(kern, C::smem, attr, "adjoint seed kernel smem attribute")) return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VqLqT, b, dt,
-                                                              j->Qbar, j->resbar, j->rhsbar,
-                                                              j->sfbar);
+  kern<<<(a->K + C::EW - 1) / C::EW, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VqLqT, b,
+                                                               dt, j->Qbar, j->resbar, j->rhsbar,
+                                                               j->sfbar);
   return ck(cudaGetLastError(), "adjoint seed kernel");
 }
 
@@ -140,17 +140,15 @@ template <int DIM, int N, bool CURVED>
 int launch_proj(const wadg_adjoint *j, cudaStream_t s, const double *Qs, double ra, double rb,
                 bool seed_next, double bn, double dtn) {
   const wadg_app *a = j->app;
-  constexpr int E = pickE(256, Elem<DIM, N>::Nq);
-  using C = AdjProjCfg<DIM, N, E>;
-  static_assert(C::smem >= sizeof(double) * 2 * E * Elem<DIM, N>::Nfields * Elem<DIM, N>::Nq,
-                "the seed reuses the projection's shared memory");
-  auto kern = seed_next ? adj_proj_kernel<DIM, N, CURVED, E, true> : adj_proj_kernel<DIM, N, CURVED, E, false>;
+  using C = AdjMmaCfg<DIM, N, CURVED>;
+  auto kern = seed_next ? adj_proj_mma_kernel<DIM, N, CURVED, true>
+                        : adj_proj_mma_kernel<DIM, N, CURVED, false>;
   static bool attr[2] = {false, false};
   if (int r = set_smem(kern, C::smem, attr[seed_next], "adjoint projection kernel smem attribute"))
     return r;
-  kern<<<(a->K + E - 1) / E, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VfPqT, Qs, j->vbar,
-                                                      j->vfbar, ra, rb, j->Qbar, j->resbar, j->phys,
-                                                      j->VqLqT, bn, dtn, j->rhsbar, j->sfbar);
+  kern<<<(a->K + C::EW - 1) / C::EW, C::threads, C::smem, s>>>(
+      a->K, a->Jq, j->VqPqT, j->VfPqT, Qs, j->vbar, j->vfbar, ra, rb, j->Qbar, j->resbar, j->phys,
+      j->VqLqT, bn, dtn, j->rhsbar, j->sfbar);
   return ck(cudaGetLastError(), "adjoint projection kernel");
 }
 

@@ -10,16 +10,19 @@
 // weight-adjusted inverse mass.  Its adjoint, given (Qbar', resbar'):
 //   r = resbar' + b Qbar',  resbar = a r,  Qbar = Qbar' + (dR/dQ)^T (dt r).
 // Three kernels evaluate it:
-//   adj_seed_kernel   w = dt r, rhsbar = Minv^T w, sfbar = VqLq^T rhsbar
-//                     (the adjoint of the lift rhsQ += VqLq sf)
-//   adj_pairs_kernel  the VJP of every two-point flux evaluation (volume-volume,
-//                     volume-face and surface, with the Lax-Friedrichs
-//                     penalty), then the adjoints of the primitive recovery
-//                     and of U(V~) at each volume and face node: vbar, vfbar
-//   adj_proj_kernel   the adjoint of the entropy projection and of V(Q), and
-//                     the LSRK adjoint update of Qbar and resbar; in a reverse
-//                     sweep it also seeds the next stage (so adj_seed_kernel
-//                     runs only for the sweep's first stage).
+//   adj_seed_mma_kernel  w = dt r, rhsbar = Minv^T w, sfbar = VqLq^T rhsbar
+//                        (the adjoint of the lift rhsQ += VqLq sf;
+//                        wadg_adjoint_mma.cuh)
+//   adj_pairs_kernel     the VJP of every two-point flux evaluation
+//                        (volume-volume, volume-face and surface, with the
+//                        Lax-Friedrichs penalty), then the adjoints of the
+//                        primitive recovery and of U(V~) at each volume and
+//                        face node: vbar, vfbar (this file)
+//   adj_proj_mma_kernel  the adjoint of the entropy projection and of V(Q), and
+//                        the LSRK adjoint update of Qbar and resbar; in a
+//                        reverse sweep it also seeds the next stage (so the
+//                        seed kernel runs only for the sweep's first stage;
+//                        wadg_adjoint_mma.cuh).
 // Neighbour contributions of the surface term are gathered, not scattered:
 // face node j adds the P-side derivative of the evaluation made at its
 // neighbour m = mapPq(j), which needs sfbar at m -- computed, for every
@@ -252,106 +255,6 @@ __device__ __forceinline__ AdjNode<DIM> adj_node(const double *q, int stride, co
 
 __device__ __forceinline__ adj::Gas gas_of(const Phys &P) {
   return adj::Gas{P.gamma, P.gm1, P.cbeta, P.lgm1, P.igm1};
-}
-
-// ------------------------------------------------------------------ seed
-// w = dt (resbar + b Qbar); rhsbar = Minv^T w; sfbar = VqLq^T rhsbar.
-//   affine Minv = -2 diag(1/J) VqPq    (Euler3Daffine.okl:555-620)
-//   WADG   Minv = VqPq diag(1/J) (-2 VqPq)   (Euler3D.okl:2527-2620)
-template <int DIM, int N, int E> struct AdjSeedCfg {
-  using El = Elem<DIM, N>;
-  static constexpr int threads = E * El::Nq;
-  static constexpr size_t smem = sizeof(double) * 2 * E * El::Nfields * El::Nq;
-};
-
-// Seed of a stage adjoint from w (this thread's node, all fields) for the
-// E elements of the block: rhsbar = Minv^T w and sfbar = VqLq^T rhsbar.
-// Called by every thread of the block (it synchronises); sA and sB are two
-// [E][Nf][Nq] shared-memory blocks.
-template <int DIM, int N, bool CURVED, int E>
-__device__ __forceinline__ void seed_block(int k0, int kend, int e, int i, bool valid,
-                                           const double *w, double Jqi,
-                                           const double *__restrict__ VqPqT,
-                                           const double *__restrict__ VqLqT, double *smem,
-                                           double *__restrict__ rhsbar,
-                                           double *__restrict__ sfbar) {
-  using El = Elem<DIM, N>;
-  constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
-  double (*sA)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
-  double (*sB)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
-  const size_t id = (size_t)(k0 + e) * Nq * Nf + i;
-
-  // transposed matvec from the stored transpose: out[f] = sum_j OpT(row, j) X[f][j]
-  // (OpT column-major with ld rows; consecutive threads read consecutive rows)
-  auto matvecT = [&](const double *OpT, int ld, int row, double (*X)[Nq], double *out) {
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) out[f] = 0.0;
-    for (int j = 0; j < Nq; ++j) {
-      const double wt = __ldg(OpT + row + j * ld);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) out[f] = fma(wt, X[f][j], out[f]);
-    }
-  };
-
-  if (valid) {
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) sA[e][f][i] = CURVED ? w[f] : -2.0 * w[f] / Jqi;
-  }
-  __syncthreads();
-  double r[Nf];
-  if (CURVED) {
-    if (valid) {
-      matvecT(VqPqT, Nq, i, sA[e], r);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) sB[e][f][i] = -2.0 * r[f] / Jqi;
-    }
-    __syncthreads();
-    if (valid) matvecT(VqPqT, Nq, i, sB[e], r);
-    __syncthreads();
-  } else if (valid) {
-    matvecT(VqPqT, Nq, i, sA[e], r);
-  }
-  if (valid) {
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) {
-      rhsbar[id + f * Nq] = r[f];
-      sB[e][f][i] = r[f];
-    }
-  }
-  __syncthreads();
-  // sfbar(f) = sum_i VqLq(i, f) rhsbar(i)
-  for (int t = threadIdx.x; t < kend * NF; t += blockDim.x) {
-    const int ee = t / NF, fn = t % NF;
-    double sv[Nf];
-    matvecT(VqLqT, NF, fn, sB[ee], sv);
-    double *out = sfbar + (size_t)(k0 + ee) * NF * Nf + fn;
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) out[f * NF] = sv[f];
-  }
-}
-
-template <int DIM, int N, bool CURVED, int E>
-__global__ void __launch_bounds__(AdjSeedCfg<DIM, N, E>::threads)
-adj_seed_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
-                const double *__restrict__ VqLqT, double b, double dt,
-                const double *__restrict__ Qbar, const double *__restrict__ resbar,
-                double *__restrict__ rhsbar, double *__restrict__ sfbar) {
-  using El = Elem<DIM, N>;
-  constexpr int Nq = El::Nq, Nf = El::Nfields;
-  extern __shared__ double smem[];
-  const int k0 = blockIdx.x * E;
-  const int kend = min(K - k0, E);
-  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
-  const bool valid = e < kend;
-  const size_t id = (size_t)k * Nq * Nf + i;
-  double w[Nf];
-  double Jqi = 1.0;
-  if (valid) {
-    Jqi = Jq[(size_t)k * Nq + i];
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) w[f] = dt * fma(b, Qbar[id + f * Nq], resbar[id + f * Nq]);
-  }
-  seed_block<DIM, N, CURVED, E>(k0, kend, e, i, valid, w, Jqi, VqPqT, VqLqT, smem, rhsbar, sfbar);
 }
 
 // ------------------------------------------------------------------ pairs
@@ -760,118 +663,6 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
         for (int f = 0; f < Nf; ++f) o[f * NF] = Vb[f];
       }
     }
-  }
-}
-
-// ------------------------------------------------------------------ projection
-// Adjoint of the entropy projection and of V(Q), then the LSRK adjoint update.
-//   affine: u~ = U(VqPq v), uf~ = U(VfPq v), v = V(Q)
-//   WADG:   v~ = VqPq((VqPq (v J)) / J), u~ = U(VqPq v~), uf~ = U(VfPq v~)
-// X = VqPq^T vbar + VfPq^T vfbar;  affine: v-bar = X;
-// WADG: v-bar = J VqPq^T((VqPq^T X) / J);  Qbar += dV/dQ^T v-bar.
-template <int DIM, int N, int E> struct AdjProjCfg {
-  using El = Elem<DIM, N>;
-  static constexpr int threads = E * El::Nq;
-  static constexpr size_t smem = sizeof(double) * E * El::Nfields * (2 * El::Nq + El::NfqNf);
-};
-
-// SEED = true: then seeds the next stage of the reverse sweep (coefficient bn,
-// step dtn) from the updated adjoints, as adj_seed_kernel would (its rhsbar
-// and sfbar are free: this stage's pair kernel has finished with them).
-template <int DIM, int N, bool CURVED, int E, bool SEED>
-__global__ void __launch_bounds__(AdjProjCfg<DIM, N, E>::threads)
-adj_proj_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPqT,
-                const double *__restrict__ VfPqT, const double *__restrict__ Qs,
-                const double *__restrict__ vbar, const double *__restrict__ vfbar, double a,
-                double b, double *__restrict__ Qbar, double *__restrict__ resbar, Phys P,
-                const double *__restrict__ VqLqT, double bn, double dtn,
-                double *__restrict__ rhsbar, double *__restrict__ sfbar) {
-  using El = Elem<DIM, N>;
-  constexpr int Nq = El::Nq, NF = El::NfqNf, Nf = El::Nfields;
-  extern __shared__ double smem[];
-  double (*sV)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem);
-  double (*sX)[Nf][Nq] = reinterpret_cast<double (*)[Nf][Nq]>(smem + E * Nf * Nq);
-  double (*sVf)[Nf][NF] = reinterpret_cast<double (*)[Nf][NF]>(smem + 2 * E * Nf * Nq);
-  const int k0 = blockIdx.x * E;
-  const int kend = min(K - k0, E);
-  {
-    const double *src = vbar + (size_t)k0 * Nf * Nq;
-    for (int t = threadIdx.x; t < kend * Nf * Nq; t += blockDim.x) (&sV[0][0][0])[t] = src[t];
-    const double *srf = vfbar + (size_t)k0 * Nf * NF;
-    for (int t = threadIdx.x; t < kend * Nf * NF; t += blockDim.x) (&sVf[0][0][0])[t] = srf[t];
-  }
-  __syncthreads();
-  const int e = threadIdx.x / Nq, i = threadIdx.x % Nq, k = k0 + e;
-  const bool valid = e < kend;
-  const double Jqi = valid ? Jq[(size_t)k * Nq + i] : 1.0;
-
-  double x[Nf];
-#pragma unroll
-  for (int f = 0; f < Nf; ++f) x[f] = 0.0;
-  if (valid) {
-    for (int j = 0; j < Nq; ++j) {
-      const double w = __ldg(VqPqT + i + j * Nq);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) x[f] = fma(w, sV[e][f][j], x[f]);
-    }
-    for (int j = 0; j < NF; ++j) {
-      const double w = __ldg(VfPqT + i + j * Nq);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) x[f] = fma(w, sVf[e][f][j], x[f]);
-    }
-  }
-  if (CURVED) {
-    // y = VqPq^T x / J ; z = VqPq^T y ; vbar = J z
-    if (valid)
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) sX[e][f][i] = x[f];
-    __syncthreads();
-    double y[Nf];
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) y[f] = 0.0;
-    if (valid) {
-      for (int j = 0; j < Nq; ++j) {
-        const double w = __ldg(VqPqT + i + j * Nq);
-#pragma unroll
-        for (int f = 0; f < Nf; ++f) y[f] = fma(w, sX[e][f][j], y[f]);
-      }
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) sV[e][f][i] = y[f] / Jqi;  // sV is free: read before the first barrier
-    }
-    __syncthreads();
-    if (valid) {
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) x[f] = 0.0;
-      for (int j = 0; j < Nq; ++j) {
-        const double w = __ldg(VqPqT + i + j * Nq);
-#pragma unroll
-        for (int f = 0; f < Nf; ++f) x[f] = fma(w, sV[e][f][j], x[f]);
-      }
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) x[f] *= Jqi;
-    }
-  }
-  const size_t id = (size_t)k * Nq * Nf + i;
-  double wn[Nf];
-  if (valid) {
-    double U[Nf], Ub[Nf];
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) U[f] = Qs[id + f * Nq];
-    adj::VU_vjp<DIM>(U, x, gas_of(P), Ub);
-#pragma unroll
-    for (int f = 0; f < Nf; ++f) {
-      const double qb = Qbar[id + f * Nq];
-      const double rt = fma(b, qb, resbar[id + f * Nq]);
-      const double rn = a * rt, qn = qb + Ub[f];
-      resbar[id + f * Nq] = rn;
-      Qbar[id + f * Nq] = qn;
-      wn[f] = dtn * fma(bn, qn, rn);
-    }
-  }
-  if (SEED) {
-    __syncthreads();  // every thread is done with sV / sX
-    seed_block<DIM, N, CURVED, E>(k0, kend, e, i, valid, wn, Jqi, VqPqT, VqLqT, smem, rhsbar,
-                                  sfbar);
   }
 }
 
