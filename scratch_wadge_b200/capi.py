@@ -318,8 +318,10 @@ class Solver:
 
     def __init__(self, mesh: M.Mesh, N: int, curved: bool, ic="taylor_green", gamma=1.4, tau=1.0,
                  ic_args=None, stream=None):
+        from .geometry_gpu import build_geometry_gpu  # (imports this module)
+
         self.mesh, self.N, self.curved, self.gamma = mesh, N, curved, gamma
-        self.geo = M.build_geometry(mesh, N)
+        self.geo = build_geometry_gpu(mesh, N)  # geometric factors and maps on the device
         self.ic, self.ic_args = ic, dict(ic_args or {})
         U0 = IC.initial_state(self.geo, ic, gamma, **self.ic_args)
         self.Q0, self.rhsQ0, self.Qf0, self.resQ0 = IC.stage0(self.geo, U0, gamma)
