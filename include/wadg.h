@@ -197,6 +197,19 @@ int wadg_match_faces(const wadg_geo_ops *ops, int K, const double *xa,
                      void *work, size_t work_bytes, uint32_t *mapPq,
                      void *stream);
 
+/* ------------------------------------------------------------ partitions
+ * Element partitioning with a face-trace halo (the exchange the reference's
+ * partitioned mesh was to do, euler.c:2468-2605, never written there).  A
+ * part keeps its neighbours' traces as ghost pseudo-elements appended to its
+ * Qf array, so the surface kernel reads them through mapPq unchanged.
+ * wadg_halo_pack fills a send buffer of n slots (a multiple of NfqNf): slot
+ * g takes the trace at field-strided index src[g] of Qf (nQf doubles), all
+ * fields, at face point g % NfqNf of pseudo-element g / NfqNf; padding slots
+ * (src = 0xffffffff) get zeros.  The buffer's blocks then go to the other
+ * parts' ghost regions (an all-to-all), between stages. */
+int wadg_halo_pack(wadg_ctx *ctx, int n, const uint32_t *src, const double *Qf,
+                   size_t nQf, double *buf);
+
 /* ------------------------------------------------------------ mesh I/O
  * The host driver's mesh files.  wadg_mesh_read_gmsh reads ASCII gmsh 2.x as
  * host_mesh_read_msh does (euler.c:556-833): the nodes; the elements of type

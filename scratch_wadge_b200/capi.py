@@ -97,6 +97,7 @@ def lib():
         L.wadg_euler_3d_compute_aux.argtypes = [v, i, v, v, v, v]
         L.wadg_element_entropy.argtypes = [v, i, v, v, v, v]
         L.wadg_entropy_rhs.argtypes = [v, i, i] + [v] * 6
+        L.wadg_halo_pack.argtypes = [v, i, v, v, ctypes.c_size_t, v]
         L.wadg_vol_warps_candidates.argtypes = [v, i, ctypes.POINTER(ctypes.c_int)]
         L.wadg_ctx_set_vol_warps.argtypes = [v, i, i]
         L.wadg_ctx_get_vol_warps.argtypes = [v]
@@ -187,6 +188,10 @@ class Context:
     def compute_aux(self, K, Jq, wq, Q, aux):
         """per-element kinetic energy (euler_3d_compute_aux)"""
         check(lib().wadg_euler_3d_compute_aux(self.h, K, Jq, wq, Q, aux), "compute_aux")
+
+    def halo_pack(self, n, src, Qf, nQf, buf):
+        """wadg_halo_pack: n send slots gathered from Qf (device pointers)"""
+        check(lib().wadg_halo_pack(self.h, n, src, Qf, nQf, buf), "halo_pack")
 
     def entropy_rhs(self, curved, K, wq, Jq, VqPq, Q, rhs, out):
         """per-element entropy balance sum_i w v~ . rhs (wadg_entropy_rhs)"""

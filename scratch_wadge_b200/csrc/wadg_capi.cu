@@ -289,6 +289,20 @@ int launch_integral(const wadg_ctx *c, int K, const double *Jq, const double *wq
   return after_launch("element integral kernel");
 }
 
+// halo pack: slot g of the send buffer gets the face trace at field-strided
+// index src[g] (all fields), laid out as the receiver's ghost pseudo-elements
+// (slot g -> face point g % NF of pseudo-element g / NF); padding slots
+// (src = 0xffffffff) and indices past the end of Qf get zeros
+__global__ void halo_pack_kernel(int n, int NF, int Nf, size_t nQf, const uint32_t *__restrict__ src,
+                                 const double *__restrict__ Qf, double *__restrict__ buf) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const uint32_t sidx = src[g];
+  const bool ok = sidx != 0xffffffffu && (size_t)sidx + (size_t)(Nf - 1) * NF < nQf;
+  double *out = buf + (size_t)(g / NF) * NF * Nf + g % NF;
+  for (int f = 0; f < Nf; ++f) out[(size_t)f * NF] = ok ? Qf[(size_t)sidx + (size_t)f * NF] : 0.0;
+}
+
 template <int DIM, int N, bool CURVED>
 int launch_entropy_rhs(const wadg_ctx *c, int K, const double *wq, const double *Jq,
                        const double *VqPq, const double *Q, const double *rhs, double *out) {
@@ -400,6 +414,17 @@ int wadg_element_entropy(wadg_ctx *c, int K, const double *Jq, const double *wq,
   if (K == 0) return WADG_OK;
   if (any_null({Jq, wq, Q, S})) return fail(WADG_ERR_INVALID, "null pointer argument");
   WADG_DISPATCH(c, return (launch_integral<D_, N_, true>(c, K, Jq, wq, Q, S)));
+}
+
+int wadg_halo_pack(wadg_ctx *c, int n, const uint32_t *src, const double *Qf, size_t nQf,
+                   double *buf) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  const int NF = c->Nfq * c->Nfaces, Nf = c->dim + 2;
+  if (n < 0 || n % NF) return fail(WADG_ERR_INVALID, "slot count must be a multiple of NfqNf");
+  if (n == 0) return WADG_OK;
+  if (any_null({src, Qf, buf})) return fail(WADG_ERR_INVALID, "null pointer argument");
+  halo_pack_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, NF, Nf, nQf, src, Qf, buf);
+  return after_launch("halo pack kernel");
 }
 
 int wadg_entropy_rhs(wadg_ctx *c, int K, int curved, const double *wq, const double *Jq,
