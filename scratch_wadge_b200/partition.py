@@ -180,17 +180,26 @@ class Part:
             self.ctx.halo_pack(n, self.send_src.data_ptr(), self.Qf.data_ptr(), self.Qf.numel(),
                                self.sendbuf.data_ptr())
 
-    def stage(self, a, b, dt):
+    def vol(self):
+        """the volume kernel (reads the part's own traces only)"""
         g, K = self.g, self.plan.K
         self.ctx.vol(self.curved, K, g["vgeo"].data_ptr(), g["vfgeo"].data_ptr(), g["nrJ"].data_ptr(),
                      g["nsJ"].data_ptr(), g["ntJ"].data_ptr(), g["Drq"].data_ptr(), g["Dsq"].data_ptr(),
                      g["Dtq"].data_ptr(), g["VqLq"].data_ptr(), g["VfPq"].data_ptr(),
                      self.Qf.data_ptr(), self.rhsQ.data_ptr(), self.rhsQf.data_ptr())
+
+    def surf_update(self, a, b, dt):
+        """the surface kernel (reads the ghosts) and the update"""
+        g, K = self.g, self.plan.K
         self.ctx.surf(K, g["fgeo"].data_ptr(), g["mapPq"].data_ptr(), g["VqLq"].data_ptr(),
                       self.Qf.data_ptr(), self.rhsQf.data_ptr(), self.rhsQ.data_ptr())
         self.ctx.update(self.curved, K, g["Jq"].data_ptr(), g["VqPq"].data_ptr(), g["VfPq"].data_ptr(),
                         a, b, dt, self.rhsQ.data_ptr(), self.resQ.data_ptr(), self.Q.data_ptr(),
                         self.Qf.data_ptr())
+
+    def stage(self, a, b, dt):
+        self.vol()
+        self.surf_update(a, b, dt)
 
     def close(self):
         self.ctx.close()
@@ -217,13 +226,15 @@ def exchange_local(parts: list) -> None:
                 pr.ghost[rb[s][0]:rb[s][1]].copy_(ps.sendbuf[sb[0]:sb[1]])
 
 
-def exchange_dist(part: Part, group=None) -> None:
+def exchange_dist(part: Part, group=None, async_op=False):
     """The all-to-all of the halo across ranks (one part per rank), between
-    stages: every rank takes it in the same order."""
+    stages: every rank takes it in the same order.  With async_op the
+    collective is queued behind the pack and the caller waits on the returned
+    work before the surface kernel."""
     import torch.distributed as dist
     part.pack()
-    dist.all_to_all_single(part.ghost, part.sendbuf, part.plan.recv_counts(),
-                           part.plan.send_counts(), group=group)
+    return dist.all_to_all_single(part.ghost, part.sendbuf, part.plan.recv_counts(),
+                                  part.plan.send_counts(), group=group, async_op=async_op)
 
 
 def run_local(parts: list, dt: float, nsteps: int) -> None:
@@ -236,11 +247,15 @@ def run_local(parts: list, dt: float, nsteps: int) -> None:
 
 
 def run_dist(part: Part, dt: float, nsteps: int, group=None) -> None:
-    """nsteps LSRK-45 time steps of this rank's part."""
+    """nsteps LSRK-45 time steps of this rank's part.  The halo exchange of a
+    stage runs while its volume kernel does (only the surface kernel reads
+    the ghosts)."""
     for _ in range(nsteps):
         for st in range(5):
-            exchange_dist(part, group)
-            part.stage(IC.RK4A[st], IC.RK4B[st], dt)
+            work = exchange_dist(part, group, async_op=True)
+            part.vol()
+            work.wait()
+            part.surf_update(IC.RK4A[st], IC.RK4B[st], dt)
 
 
 def gather_Q(parts: list, K: int) -> np.ndarray:
