@@ -8,12 +8,13 @@ import os
 import numpy as np
 import pytest
 
+from oracle.build import REF_DIR
 from scratch_wadge_b200 import build as B
 from scratch_wadge_b200 import capi
 from scratch_wadge_b200 import mesh as M
 from scratch_wadge_b200 import meshio as IO
 
-REF_MESHES = "/root/reference/meshes"
+REF_MESHES = os.path.join(REF_DIR, "meshes")
 
 
 @pytest.fixture(scope="module", autouse=True)
