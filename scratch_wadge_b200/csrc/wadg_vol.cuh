@@ -23,7 +23,9 @@
 //
 // Persistent CTAs: operator tables are staged in shared memory once per CTA;
 // the face weights in a rotated layout [r][s][l] so that the lanes of a step
-// read consecutive words.
+// read consecutive words.  In the volume kernel's batch loop the warps of an
+// element group synchronise only among themselves (named barriers): a
+// group's shared memory is its own, so no group waits for another.
 #pragma once
 
 #include "wadg_device.cuh"
@@ -142,10 +144,22 @@ struct VolPairs {
   __device__ __forceinline__ void prologue(int K, int k0, const double *vgeo, const double *vfgeo,
                                            const double *uq, const double *uf, const Phys &P,
                                            const double *ufs = nullptr) {
-    for (int t = tid; t < E * NN; t += blockDim.x) {
-      const int ee = t / NN, n = t % NN;
+    prologue_range(K, k0, 0, E, tid, blockDim.x, vgeo, vfgeo, uq, uf, P, ufs);
+  }
+
+  // the same for the batch elements [e0, e0 + ne), by threads t0, t0 + ts, ...
+  __device__ __forceinline__ void prologue_range(int K, int k0, int e0, int ne, int t0, int ts,
+                                                 const double *vgeo, const double *vfgeo,
+                                                 const double *uq, const double *uf,
+                                                 const Phys &P, const double *ufs) {
+    for (int t = t0; t < ne * NN; t += ts) {
+      const int ee = e0 + t / NN, n = t % NN;
       const int k = min(k0 + ee, K - 1);
-      const double *fsrc = ufs ? ufs + (size_t)(k - k0) * NF * Nf : uf + (size_t)k * NF * Nf;
+      // staged traces only for this range's own elements (a clamped element's
+      // copy may sit in another range, staged by other threads)
+      const int kk = k - k0;
+      const double *fsrc = (ufs && kk >= e0 && kk < e0 + ne) ? ufs + (size_t)kk * NF * Nf
+                                                             : uf + (size_t)k * NF * Nf;
       const NodeState<DIM> s = (n < Nq) ? node_state<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
                                         : node_state<DIM>(fsrc + (n - Nq), NF, P);
       double *st = sSt + ee * SE;
@@ -162,9 +176,9 @@ struct VolPairs {
                                            : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
       }
     }
-    for (int t = tid; t < E * SA; t += blockDim.x) sAcc[t] = 0.0;
+    for (int t = t0; t < ne * SA; t += ts) sAcc[e0 * SA + t] = 0.0;
     if (!CURVED) {
-      for (int t = tid; t < E; t += blockDim.x) {
+      for (int t = e0 + t0; t < e0 + ne; t += ts) {
         const int k = min(k0 + t, K - 1);
         double Gk[NG];
 #pragma unroll
@@ -323,28 +337,44 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
   V v(smem);
   v.load_tables(nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq);
   constexpr bool PRE = V::C::PREFETCH;
-  // stage batch kb's face traces (a contiguous range of Qf) into shared memory
-  auto prefetch = [&](int kb) {
-    if (kb < K) {
-      const int n = min(K - kb, E) * NF * Nf;
-      const double *src = Qf + (size_t)kb * NF * Nf;
-      for (int t = threadIdx.x; t < n; t += blockDim.x) cp_async8(v.sPre + t, src + t);
+  // After the tables, the H warps of an element group touch only their own
+  // G elements' shared memory (states, face rows, normals, staged traces),
+  // so within the batch loop they synchronise among themselves (a named
+  // barrier per group) and never wait for the CTA's other groups.
+  constexpr int G = V::G, GT = 32 * H;
+  const int q = (threadIdx.x >> 5) / H, tq = threadIdx.x - q * GT;
+  auto gsync = [&] {
+    if (H == 1)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;\n" ::"r"(1 + q), "r"(GT) : "memory");
+  };
+  // stage the group's elements of batch kb (face traces, a contiguous range
+  // of Qf) into shared memory
+  auto prefetch_group = [&](int kb) {
+    const int kq = kb + q * G;
+    if (kq < K) {
+      const int n = min(K - kq, G) * NF * Nf;
+      const double *src = Qf + (size_t)kq * NF * Nf;
+      double *dst = v.sPre + (size_t)q * G * NF * Nf;
+      for (int t = tq; t < n; t += GT) cp_async8(dst + t, src + t);
     }
     cp_async_commit();
   };
-  if (PRE) prefetch(blockIdx.x * E);
+  __syncthreads();  // the tables are shared by every group
+  if (PRE) prefetch_group(blockIdx.x * E);
 
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
     if (PRE) cp_async_wait_all();
-    __syncthreads();  // tables ready / previous batch done with shared memory / traces staged
-    v.prologue(K, k0, vgeo, vfgeo, rhsQ, Qf, P, PRE ? v.sPre : nullptr);
-    __syncthreads();
-    if (PRE) prefetch(k0 + gridDim.x * E);  // the next batch's traces, during the pairs
+    gsync();  // the group's traces staged / its previous batch done with its shared memory
+    v.prologue_range(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P, PRE ? v.sPre : nullptr);
+    gsync();
+    if (PRE) prefetch_group(k0 + gridDim.x * E);  // the next batch's traces, during the pairs
     double acc[R][Nf];
     v.pairs(acc, P);
-    __syncthreads();  // all pairs done: the state block becomes the row buffer
+    gsync();  // the group's pairs done: its state block becomes the row buffer
     v.park_rows(acc);
-    __syncthreads();
+    gsync();
     const int k = k0 + v.e;
     if (k < K) {
       const double *rowbuf = v.sSt + v.e * V::SE;
