@@ -374,24 +374,43 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
   const adj::Gas gas = gas_of(P);
 
   constexpr bool PRE = C::PREFETCH;
+  // After the tables, the H warps of an element group touch only their own
+  // G elements' shared memory, so within the batch loop they synchronise
+  // among themselves (a named barrier per group), never with other groups.
+  const int q = warp / H, tq = tid - q * 32 * H, e0 = q * G;
+  constexpr int GT = 32 * H;
+  auto gsync = [&] {
+    if (H == 1)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;\n" ::"r"(1 + q), "r"(GT) : "memory");
+  };
+  // stage the group's elements of batch kb (face traces) into shared memory
   auto prefetch = [&](int kb) {
-    if (kb < K) {
-      const int n = min(K - kb, E) * NF * Nf;
-      const double *src = uf + (size_t)kb * NF * Nf;
-      for (int t = tid; t < n; t += blockDim.x) cp_async8(sPre + t, src + t);
+    const int kq = kb + e0;
+    if (kq < K) {
+      const int n = min(K - kq, G) * NF * Nf;
+      const double *src = uf + (size_t)kq * NF * Nf;
+      double *dst = sPre + (size_t)e0 * NF * Nf;
+      for (int t = tq; t < n; t += GT) cp_async8(dst + t, src + t);
     }
     cp_async_commit();
   };
+  __syncthreads();  // the tables are shared by every group
   if (PRE) prefetch(blockIdx.x * E);
 
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
     if (PRE) cp_async_wait_all();
-    __syncthreads();  // tables ready / previous batch done with shared memory / traces staged
+    gsync();  // the group's traces staged / its previous batch done with its shared memory
     // ---- prologue: node states, face seeds, zeroed column adjoints, normals
-    for (int t = tid; t < E * NN; t += blockDim.x) {
-      const int ee = t / NN, n = t % NN;
+    for (int t = tq; t < G * NN; t += GT) {
+      const int ee = e0 + t / NN, n = t % NN;
       const int k = min(k0 + ee, K - 1);
-      const double *fsrc = PRE ? sPre + (size_t)(k - k0) * NF * Nf : uf + (size_t)k * NF * Nf;
+      // staged traces only for the group's own elements (a clamped element's
+      // copy may sit in another group's range)
+      const int kk = k - k0;
+      const double *fsrc = (PRE && kk >= e0 && kk < e0 + G) ? sPre + (size_t)kk * NF * Nf
+                                                            : uf + (size_t)k * NF * Nf;
       const AdjNode<DIM> s = (n < Nq) ? adj_node<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
                                       : adj_node<DIM>(fsrc + (n - Nq), NF, P);
       double *st = sEl + ee * C::per_elem;
@@ -410,17 +429,17 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
                                             : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
       }
     }
-    for (int t = tid; t < E * C::SSF; t += blockDim.x) {
-      const int ee = t / C::SSF, u = t % C::SSF;
+    for (int t = tq; t < G * C::SSF; t += GT) {
+      const int ee = e0 + t / C::SSF, u = t % C::SSF;
       const int k = min(k0 + ee, K - 1);
       sEl[ee * C::per_elem + C::SST + u] = sfbar[(size_t)k * NF * Nf + u];
     }
-    for (int t = tid; t < E * C::SBR; t += blockDim.x) {
-      const int ee = t / C::SBR, u = t % C::SBR;
+    for (int t = tq; t < G * C::SBR; t += GT) {
+      const int ee = e0 + t / C::SBR, u = t % C::SBR;
       sEl[ee * C::per_elem + C::SST + C::SSF + u] = 0.0;
     }
     if (!CURVED) {
-      for (int t = tid; t < E; t += blockDim.x) {
+      for (int t = e0 + tq; t < e0 + G; t += GT) {
         const int k = min(k0 + t, K - 1);
         double Gk[NG];
 #pragma unroll
@@ -438,7 +457,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           }
       }
     }
-    __syncthreads();
+    gsync();
     if (PRE) prefetch(k0 + gridDim.x * E);  // the next batch's traces, during the pairs
 
     // ---- pairs
@@ -562,7 +581,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     // row adjoints into the column adjoints, one warp of the element at a time
 #pragma unroll
     for (int hh = 0; hh < H; ++hh) {
-      __syncthreads();
+      gsync();
       if (h == hh) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -574,11 +593,11 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
         }
       }
     }
-    __syncthreads();
+    gsync();
 
     // ---- per node: surface term (face nodes), primitive recovery and U(V~) adjoints
-    for (int t = tid; t < E * NN; t += blockDim.x) {
-      const int ee = t / NN, n = t % NN, k = k0 + ee;
+    for (int t = tq; t < G * NN; t += GT) {
+      const int ee = e0 + t / NN, n = t % NN, k = k0 + ee;
       if (k >= K) continue;
       const double *ste = sEl + ee * C::per_elem;
       const double *bt = ste + C::SST + C::SSF;
