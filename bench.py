@@ -4,8 +4,8 @@ Workload (one "step" = one LSRK-45 time step = 5 stages x {vol, surf, update}):
   3D Taylor-Green vortex on affine tetrahedra (Euler3Daffine kernels), FP64,
   periodic [-pi,pi]^3, 16^3 hexes x 6 tets = 24576 elements, N = 3,
   gamma = 1.4, CFL 0.5 (dt = CFL hmin / (C_N max(|u|+c)); the reference's
-  formula without the wave speed is unstable on this state).  Synthetic: the mesh and the initial state are
-  generated here (no external data).
+  formula without the wave speed is unstable on this state).  Synthetic: the
+  mesh and the initial state are generated here (no external data).
 Metric: FP64 DOF*stages/s, DOF = K * Np per field (Np = 20, Nfields = 5).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -18,7 +18,13 @@ one (`roofline`, `hbm_kernels`).  Two more workloads are reported beside the
 headline: `ensemble` (256 independent 2D vortex solves, batched against one
 solver per instance) and `adjoint` (the checkpointed discrete adjoint of a
 200-step Taylor-Green run on 3072 tets: reverse-sweep cost over the forward
-run, and a finite-difference check of the gradient).
+run, and a finite-difference check of the gradient).  `setup` compares the
+geometry builders on the workload mesh (GPU: wadg_geofacs + wadg_match_faces;
+host: numpy).
+
+Multi-GPU runs are replicas: the headline path is single-rank (the
+reference's rk_step exchanges nothing).  Partitioned solves with a halo
+exchange are scratch_wadge_b200/partition.py (not benchmarked here).
 
 --impl ours       the CUDA library through its C ABI; `value` is timed with
                   CUDA events around K graph-replayed time steps with the state
