@@ -69,3 +69,24 @@ def test_supported_degrees(L):
             p = capi.params_for(ops)
             assert L.wadg_ctx_create(ctypes.byref(p), ctypes.byref(h)) == 0
             L.wadg_ctx_destroy(h)
+
+
+def test_diagnostic_and_halo_validation(L):
+    """wadg_entropy_rhs and wadg_halo_pack reject bad arguments before any
+    CUDA call; empty work is a no-op."""
+    ops = R.load(3, 3)
+    h = ctypes.c_void_p()
+    p = capi.params_for(ops)
+    assert L.wadg_ctx_create(ctypes.byref(p), ctypes.byref(h)) == 0
+    # entropy balance: K < 0, K = 0, null arrays, curved without Jq
+    assert L.wadg_entropy_rhs(h, -1, 0, *([None] * 6)) == 1
+    assert L.wadg_entropy_rhs(h, 0, 0, *([None] * 6)) == 0
+    assert L.wadg_entropy_rhs(h, 4, 0, *([None] * 6)) == 1
+    assert L.wadg_entropy_rhs(h, 4, 1, 8, None, 8, 8, 8, 8) == 1  # curved reads Jq
+    # halo pack: slot counts must be whole pseudo-elements (NfqNf = 48)
+    assert L.wadg_halo_pack(h, 0, None, None, 0, None) == 0
+    assert L.wadg_halo_pack(h, 47, 8, 8, 100, 8) == 1
+    assert b"multiple" in L.wadg_last_error()
+    assert L.wadg_halo_pack(h, -48, 8, 8, 100, 8) == 1
+    assert L.wadg_halo_pack(h, 48, None, 8, 100, 8) == 1
+    L.wadg_ctx_destroy(h)
