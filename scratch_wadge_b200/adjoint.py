@@ -127,3 +127,41 @@ def rho2_objective(geo, Q: torch.Tensor):
     g = torch.zeros_like(Q)
     g[:, 0, :] = 2.0 * w * rho
     return J, g
+
+
+def main(argv=None):
+    """Gradient of J = int rho(T)^2 for a periodic Taylor-Green cube, N=3:
+    forward run with checkpoints, then the reverse sweep, `repeat` times
+    (a small case for profilers).
+
+        python -m scratch_wadge_b200.adjoint --cube 8 --steps 2 --every 2
+    """
+    import argparse
+
+    from . import ic as IC
+    from . import mesh as M
+
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n")[0])
+    ap.add_argument("--cube", type=int, default=8, help="hexes per direction (6 tets each)")
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--every", type=int, default=2, help="checkpoint every this many steps")
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args(argv)
+    geo = M.build_geometry(M.periodic_cube(a.cube), 3)
+    Q0 = IC.stage0(geo, IC.initial_state(geo, "taylor_green"))[0]
+    dt = IC.time_step(geo, 0.5, 3, nsteps=200, wave_speed=IC.max_wave_speed(Q0))[0]
+    app = capi.App(geo, False)
+    adj = Adjoint(app, a.steps, a.every)
+    Qd = torch.from_numpy(Q0).cuda()
+    for _ in range(a.repeat):
+        QT = adj.forward(Qd, dt)
+        J, gT = rho2_objective(geo, QT)
+        g = adj.reverse(gT)
+    torch.cuda.synchronize()
+    print(f"K={geo.K} steps={a.steps} J={float(J):.15g} max|dJ/dQ0|={float(g.abs().max()):.6e}")
+    adj.close()
+    app.close()
+
+
+if __name__ == "__main__":
+    main()
