@@ -425,21 +425,32 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
   extern __shared__ double smem[];
   V v(smem);
   v.load_tables(nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq);
-  const int tid = threadIdx.x, nth = blockDim.x;
+  // as in vol_pairs_kernel, an element group's warps synchronise only among
+  // themselves after the tables: every phase below touches only the group's
+  // own elements' shared memory
+  constexpr int G = V::G, GT = 32 * H;
+  const int q = (threadIdx.x >> 5) / H, tid = threadIdx.x - q * GT, nth = GT, e0 = q * G;
+  auto gsync = [&] {
+    if (H == 1)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;\n" ::"r"(1 + q), "r"(GT) : "memory");
+  };
+  __syncthreads();  // the tables are shared by every group
 
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
-    __syncthreads();
-    v.prologue(K, k0, vgeo, vfgeo, uq, uf, P);
-    __syncthreads();
+    gsync();
+    v.prologue_range(K, k0, e0, G, tid, nth, vgeo, vfgeo, uq, uf, P, nullptr);
+    gsync();
     double acc[R][Nf];
     v.pairs(acc, P);
-    __syncthreads();
+    gsync();
 
     // ---- surface: sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam) sJ (u+ - u-)
     // (Euler3D.okl:3256-3346, Euler2D.okl:1373-1453); stored over the face
     // accumulators
-    for (int t = tid; t < E * NF; t += nth) {
-      const int ee = t / NF, f = t % NF, k = k0 + ee;
+    for (int t = tid; t < G * NF; t += nth) {
+      const int ee = e0 + t / NF, f = t % NF, k = k0 + ee;
       if (k >= K) continue;
       const size_t idM = f + (size_t)k * NF * Nf;
       const size_t idP = mapPq[f + (size_t)k * NF];
@@ -477,7 +488,7 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
 #pragma unroll
       for (int q = 0; q < Nf; ++q) a0[q * NF + f] = a0[q * NF + f] + 0.5 * F[q] - Lfc * (UP[q] - UM[q]);
     }
-    __syncthreads();
+    gsync();
 
     // ---- lift: rows += VqLq sfS, on the rotated weights (VqLq = 2 W1),
     // the two warps splitting the face nodes as in the pair phase
@@ -498,7 +509,7 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
       }
     }
     v.park_rows(acc);  // the state block is free after the surface phase
-    __syncthreads();
+    gsync();
     if (v.h == 0) {
       double *rowbuf = v.sSt + v.e * SE;
 #pragma unroll
@@ -511,7 +522,7 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
         }
       }
     }
-    __syncthreads();
+    gsync();
 
     // ---- update (Euler3Daffine.okl:555-773 / Euler3D.okl:2527-2884):
     // staging per element in its state block: [0] rhs, [1] sA, [2] sB
@@ -526,8 +537,8 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
       }
     };
     if (CURVED) {
-      for (int t = tid; t < E * Nq; t += nth) {
-        const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+      for (int t = tid; t < G * Nq; t += nth) {
+        const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
         if (k >= K) continue;
         double r[Nf];
         matvec(VqPq, Nq, i, blk(ee, 0), r);
@@ -535,10 +546,10 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
 #pragma unroll
         for (int q = 0; q < Nf; ++q) blk(ee, 1)[q * Nq + i] = -2.0 * r[q] / Jqi;
       }
-      __syncthreads();
+      gsync();
     }
-    for (int t = tid; t < E * Nq; t += nth) {
-      const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+    for (int t = tid; t < G * Nq; t += nth) {
+      const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
       if (k >= K) continue;
       const double Jqi = Jq[(size_t)k * Nq + i];
       double r[Nf], U[Nf], Vv[Nf];
@@ -561,12 +572,12 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
 #pragma unroll
       for (int q = 0; q < Nf; ++q) blk(ee, 2)[q * Nq + i] = CURVED ? Vv[q] * Jqi : Vv[q];
     }
-    __syncthreads();
+    gsync();
     int src = 2;  // block holding the projected entropy variables' source
     if (CURVED) {
       // weight-adjusted projection VqPq((VqPq (v J)) / J)
-      for (int t = tid; t < E * Nq; t += nth) {
-        const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+      for (int t = tid; t < G * Nq; t += nth) {
+        const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
         if (k >= K) continue;
         double r[Nf];
         matvec(VqPq, Nq, i, blk(ee, 2), r);
@@ -574,20 +585,20 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
 #pragma unroll
         for (int q = 0; q < Nf; ++q) blk(ee, 1)[q * Nq + i] = r[q] / Jqi;
       }
-      __syncthreads();
-      for (int t = tid; t < E * Nq; t += nth) {
-        const int ee = t / Nq, i = t % Nq, k = k0 + ee;
+      gsync();
+      for (int t = tid; t < G * Nq; t += nth) {
+        const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
         if (k >= K) continue;
         double r[Nf];
         matvec(VqPq, Nq, i, blk(ee, 1), r);
 #pragma unroll
         for (int q = 0; q < Nf; ++q) blk(ee, 0)[q * Nq + i] = r[q];
       }
-      __syncthreads();
+      gsync();
       src = 0;
     }
-    for (int t = tid; t < E * (NF + Nq); t += nth) {
-      const int ee = t / (NF + Nq), n = t % (NF + Nq), k = k0 + ee;
+    for (int t = tid; t < G * (NF + Nq); t += nth) {
+      const int ee = e0 + t / (NF + Nq), n = t % (NF + Nq), k = k0 + ee;
       if (k >= K) continue;
       double Vv[Nf], U[Nf];
       if (n < NF) {
