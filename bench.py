@@ -29,9 +29,9 @@ exchange are scratch_wadge_b200/partition.py (not benchmarked here).
 --impl ours       the CUDA library through its C ABI; `value` is timed with
                   CUDA events around K graph-replayed time steps with the state
                   resident in HBM (working set ~0.3 GB > L2); `e2e` is the
-                  user-level host-buffer solve (wadg_app_solve_host: H2D of the
-                  stage-0 state from pinned memory, the config's 100 time
-                  steps, D2H of Q).  Multi-GPU: independent replicas (the path
+                  user-level host-buffer solve (wadg_app_solve_host_q: H2D of
+                  Q0 from pinned memory, the stage-0 projection on the device,
+                  the config's 100 time steps, D2H of Q).  Multi-GPU: independent replicas (the path
                   has no data exchange), max time over ranks.
 --impl reference  the reference's own kernels compiled from its OKL sources
                   (oracle/_ref, OpenMP over all host cores; the C restatement
@@ -327,21 +327,21 @@ def run_ours(args):
         "note": "the reference-facing kernels one by one, CUDA events around each launch"}
 
     # end to end through the user-level host-buffer call
-    pin = {k: torch.from_numpy(v).pin_memory() for k, v in st0.items()}
+    pin = {"Q": torch.from_numpy(st0["Q"]).pin_memory()}
     Qout = torch.empty(pin["Q"].shape, dtype=torch.float64).pin_memory()
     host = {k: v.numpy() for k, v in pin.items()}
     qo = Qout.numpy()
-    app.solve_host(host["Q"], host["rhsQ"], host["Qf"], dt, 2, resQ0=host["resQ"], out=qo)  # warm
+    app.solve_host_q(host["Q"], dt, 2, out=qo)  # warm
     barrier()
     e2e_calls = max(1, args.e2e_calls)
     t0 = time.perf_counter()
     for _ in range(e2e_calls):
-        app.solve_host(host["Q"], host["rhsQ"], host["Qf"], dt, E2E_STEPS, resQ0=host["resQ"], out=qo)
+        app.solve_host_q(host["Q"], dt, E2E_STEPS, out=qo)
     barrier()
     e2e_s = time.perf_counter() - t0
     e2e_s = RP.all_max(pg, e2e_s)
     e2e_v = RP.job_throughput(ws, dofs * 5 * E2E_STEPS * e2e_calls, e2e_s)
-    h2d = sum(v.nbytes for v in host.values())
+    h2d = host["Q"].nbytes
     d2h = qo.nbytes
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -350,8 +350,9 @@ def run_ours(args):
             "config": config_dict(geo, ws),
             "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "step": f"one wadg_app_solve_host call: H2D stage-0 state, {E2E_STEPS} time "
-                            f"steps, D2H Q (pinned host buffers, wall clock)",
+                    "step": f"one wadg_app_solve_host_q call: H2D of Q0, the stage-0 projection "
+                            f"on the device, {E2E_STEPS} time steps, D2H of Q (pinned host "
+                            f"buffers, wall clock)",
                     "calls": e2e_calls},
             "gpu_launches": (5 if use_fused else 15) * args.steps,
             "autotune": {"vol_warps": vol_warps,

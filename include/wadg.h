@@ -330,6 +330,17 @@ int wadg_app_solve_host(wadg_app *app, const double *Q0, const double *rhsQ0,
                         const double *Qf0, const double *resQ0, double dt,
                         int nsteps, double *Q, double *rhsQ, double *Qf,
                         double *resQ);
+/* The entropy projection of the app's Q into the traces the next stage
+ * reads (rhsQ = U(VqPq v), Qf = U(VfPq v), v = V(Q); curved: the
+ * weight-adjusted projection of the update kernel), and resQ = 0: the
+ * stage-0 state the reference's driver builds on the host
+ * (euler.c:3958-4133; its curved path projects with VqPq alone).
+ * Asynchronous. */
+int wadg_app_project(wadg_app *app);
+/* The user-level solve from the conserved state alone: copy Q0 in, project
+ * (wadg_app_project), run nsteps, copy Q out.  Synchronous. */
+int wadg_app_solve_host_q(wadg_app *app, const double *Q0, double dt,
+                          int nsteps, double *Q);
 int wadg_app_sync(wadg_app *app);
 /* fused != 0: wadg_rk_step / wadg_rk_run launch the fused stage kernel (one
  * launch per stage, ping-pong state buffers); 0 (the default): the three

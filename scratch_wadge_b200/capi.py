@@ -70,6 +70,8 @@ def lib():
         L.wadg_app_time_run.argtypes = [v, d, i, i, ctypes.POINTER(ctypes.c_float)]
         L.wadg_app_time_kernels.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
         L.wadg_app_solve_host.argtypes = [v, v, v, v, v, d, i, v, v, v, v]
+        L.wadg_app_solve_host_q.argtypes = [v, v, d, i, v]
+        L.wadg_app_project.argtypes = [v]
         L.wadg_app_set_state.argtypes = [v, v, v, v, v]
         L.wadg_app_get_state.argtypes = [v, v, v, v, v]
         L.wadg_app_state_ptrs.argtypes = [v] + [ctypes.POINTER(ctypes.c_void_p)] * 5
@@ -283,6 +285,19 @@ class App:
         check(lib().wadg_app_solve_host(self.h, c(Q0), c(rhsQ0), c(Qf0), c(resQ0), dt, nsteps,
                                         Q.ctypes.data, None, None, None), "solve_host")
         return Q
+
+    def solve_host_q(self, Q0, dt, nsteps, out=None):
+        """User-level solve from the conserved state alone (H2D of Q0, the
+        stage-0 projection on the device, nsteps, D2H of Q)."""
+        Q = out if out is not None else np.empty(self.vshape)
+        Q0 = np.ascontiguousarray(Q0, dtype=np.float64)
+        check(lib().wadg_app_solve_host_q(self.h, Q0.ctypes.data, dt, nsteps, Q.ctypes.data),
+              "solve_host_q")
+        return Q
+
+    def project(self):
+        """stage-0 traces and resQ = 0 from the app's Q, on the device"""
+        check(lib().wadg_app_project(self.h), "project")
 
     def time_run(self, dt, nsteps, graph=True):
         ms = ctypes.c_float()

@@ -326,6 +326,36 @@ int wadg_app_solve_host(wadg_app *a, const double *Q0, const double *rhsQ0, cons
   return wadg_app_get_state(a, Q, rhsQ, Qf, resQ);
 }
 
+int wadg_app_project(wadg_app *a) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  // the update kernel with a zero RHS and zero coefficients: Q unchanged,
+  // resQ = 0, the traces = the entropy projection of Q
+  const size_t nvb = (size_t)a->K * a->Nq * a->Nf * sizeof(double);
+  double *uq = a->uq[a->cur], *uf = a->uf[a->cur];
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(uq, 0, nvb, a->stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(a->resQ, 0, nvb, a->stream)) != cudaSuccess)
+    return afail(WADG_ERR_CUDA, "memset", e);
+  if (a->p.dim == 3)
+    return a->curved ? wadg_euler_update_3d_curved(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0,
+                                                   0.0, uq, a->resQ, a->Q, uf)
+                     : wadg_euler_update_3d(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0, 0.0, uq,
+                                            a->resQ, a->Q, uf);
+  return a->curved ? wadg_euler_update_2d_curved(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0,
+                                                 0.0, uq, a->resQ, a->Q, uf)
+                   : wadg_euler_update_2d(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0, 0.0, uq,
+                                          a->resQ, a->Q, uf);
+}
+
+int wadg_app_solve_host_q(wadg_app *a, const double *Q0, double dt, int nsteps, double *Q) {
+  if (!a || !Q0 || !Q) return afail(WADG_ERR_INVALID, "invalid argument");
+  int r = wadg_app_set_state(a, Q0, nullptr, nullptr, nullptr);
+  if (!r) r = wadg_app_project(a);
+  if (!r) r = wadg_rk_run(a, dt, nsteps, 1);
+  if (!r) r = wadg_app_get_state(a, Q, nullptr, nullptr, nullptr);
+  return r;
+}
+
 int wadg_app_sync(wadg_app *a) {
   if (!a) return afail(WADG_ERR_INVALID, "null app");
   cudaError_t e = cudaStreamSynchronize(a->stream);

@@ -233,6 +233,29 @@ def test_entropy_dissipation_2d(cuda):
     assert S > 0
 
 
+@pytest.mark.parametrize("name", ["tg3d_affine_N3", "tg3d_affine_N2", "vortex2d_affine_N2"])
+def test_device_projection_matches_stage0(cuda, name):
+    """wadg_app_project = the reference's stage-0 builder (affine meshes)."""
+    c = Case(name)
+    app = capi.App(c.geo, c.curved)
+    st = c.state()
+    app.set_state(st["Q"], st["rhsQ"] * 0 + 1.0, st["Qf"] * 0 + 1.0, st["resQ"] + 1.0)
+    app.project()
+    out = app.get_state()
+    assert rel(out["rhsQ"], st["rhsQ"]) < RTOL and rel(out["Qf"], st["Qf"]) < RTOL
+    assert np.array_equal(out["Q"], st["Q"]) and not out["resQ"].any()
+
+
+@pytest.mark.parametrize("name", ["tg3d_affine_N3", "vortex2d_affine_N2"])
+def test_solve_from_q_equals_solve_from_stage0_state(cuda, name):
+    c = Case(name)
+    app = capi.App(c.geo, c.curved)
+    st = c.state()
+    a = app.solve_host(st["Q"], st["rhsQ"], st["Qf"], c.dt, 4)
+    b = app.solve_host_q(st["Q"], c.dt, 4)
+    assert rel(b, a) < RTOL
+
+
 def test_solve_host_equals_device_run(cuda):
     c = Case("tg3d_affine_N3")
     app = capi.App(c.geo, c.curved)
