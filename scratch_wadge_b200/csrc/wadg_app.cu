@@ -59,39 +59,50 @@ void free_all(wadg_app *a) {
   if (a->own_stream && a->stream) cudaStreamDestroy(a->stream);
 }
 
-// the three reference kernels on the current buffers (rk_step, euler.c:3610)
-int stage3(wadg_app *a, double rka, double rkb, double dt) {
-  int r;
+// the reference's kernels on the current buffers (rk_step, euler.c:3610)
+int vol(wadg_app *a) {
   const int K = a->K;
   double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
-  if (a->p.dim == 3) {
-    r = a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
-                                             a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq,
-                                             a->Q, Qf, rhsQ, a->rhsQf)
-                  : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ, a->Drq,
-                                      a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q, Qf,
-                                      rhsQ, a->rhsQf);
-    if (r) return r;
-    r = wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf, a->rhsQf, rhsQ);
-    if (r) return r;
-    r = a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                                rhsQ, a->resQ, a->Q, Qf)
-                  : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, rhsQ,
-                                         a->resQ, a->Q, Qf);
-  } else {
-    r = a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
-                                             a->Dsq, a->VqLq, a->VfPq, a->Q, Qf, rhsQ,
-                                             a->rhsQf)
-                  : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq, a->Dsq,
-                                      a->VqLq, a->VfPq, a->Q, Qf, rhsQ, a->rhsQf);
-    if (r) return r;
-    r = wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf, a->rhsQf, rhsQ);
-    if (r) return r;
-    r = a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                                rhsQ, a->resQ, a->Q, Qf)
-                  : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, rhsQ,
-                                         a->resQ, a->Q, Qf);
-  }
+  if (a->p.dim == 3)
+    return a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
+                                                a->ntJ, a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq,
+                                                a->VfPq, a->Q, Qf, rhsQ, a->rhsQf)
+                     : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
+                                         a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q,
+                                         Qf, rhsQ, a->rhsQf);
+  return a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
+                                              a->Drq, a->Dsq, a->VqLq, a->VfPq, a->Q, Qf, rhsQ,
+                                              a->rhsQf)
+                   : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
+                                       a->Dsq, a->VqLq, a->VfPq, a->Q, Qf, rhsQ, a->rhsQf);
+}
+
+int surf(wadg_app *a) {
+  double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
+  return a->p.dim == 3 ? wadg_euler_surf_3d(a->ctx, a->K, a->fgeo, a->mapPq, a->VqLq, Qf,
+                                            a->rhsQf, rhsQ)
+                       : wadg_euler_surf_2d(a->ctx, a->K, a->fgeo, a->mapPq, a->VqLq, Qf,
+                                            a->rhsQf, rhsQ);
+}
+
+int update(wadg_app *a, double rka, double rkb, double dt) {
+  const int K = a->K;
+  double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
+  if (a->p.dim == 3)
+    return a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
+                                                   dt, rhsQ, a->resQ, a->Q, Qf)
+                     : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+                                            rhsQ, a->resQ, a->Q, Qf);
+  return a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+                                                 rhsQ, a->resQ, a->Q, Qf)
+                   : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, rhsQ,
+                                          a->resQ, a->Q, Qf);
+}
+
+int stage3(wadg_app *a, double rka, double rkb, double dt) {
+  int r = vol(a);
+  if (!r) r = surf(a);
+  if (!r) r = update(a, rka, rkb, dt);
   return r;
 }
 
@@ -331,20 +342,11 @@ int wadg_app_project(wadg_app *a) {
   // the update kernel with a zero RHS and zero coefficients: Q unchanged,
   // resQ = 0, the traces = the entropy projection of Q
   const size_t nvb = (size_t)a->K * a->Nq * a->Nf * sizeof(double);
-  double *uq = a->uq[a->cur], *uf = a->uf[a->cur];
   cudaError_t e;
-  if ((e = cudaMemsetAsync(uq, 0, nvb, a->stream)) != cudaSuccess ||
+  if ((e = cudaMemsetAsync(a->uq[a->cur], 0, nvb, a->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(a->resQ, 0, nvb, a->stream)) != cudaSuccess)
     return afail(WADG_ERR_CUDA, "memset", e);
-  if (a->p.dim == 3)
-    return a->curved ? wadg_euler_update_3d_curved(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0,
-                                                   0.0, uq, a->resQ, a->Q, uf)
-                     : wadg_euler_update_3d(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0, 0.0, uq,
-                                            a->resQ, a->Q, uf);
-  return a->curved ? wadg_euler_update_2d_curved(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0,
-                                                 0.0, uq, a->resQ, a->Q, uf)
-                   : wadg_euler_update_2d(a->ctx, a->K, a->Jq, a->VqPq, a->VfPq, 0.0, 0.0, 0.0, uq,
-                                          a->resQ, a->Q, uf);
+  return update(a, 0.0, 0.0, 0.0);
 }
 
 int wadg_app_solve_host_q(wadg_app *a, const double *Q0, double dt, int nsteps, double *Q) {
@@ -403,8 +405,6 @@ int wadg_app_time_run(wadg_app *a, double dt, int nsteps, int use_graph, float *
 
 int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
   if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
-  const int K = a->K;
-  double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
   cudaEvent_t ev[4];
   for (auto &x : ev) cudaEventCreate(&x);
   float tot[3] = {0, 0, 0};
@@ -412,38 +412,11 @@ int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
   for (int s = 0; s < nstages && r == WADG_OK; ++s) {
     const double rka = RK4A[s % 5], rkb = RK4B[s % 5];
     cudaEventRecord(ev[0], a->stream);
-    if (a->p.dim == 3)
-      r = a->curved ? wadg_euler_vol_3d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
-                                               a->ntJ, a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq,
-                                               a->VfPq, a->Q, Qf, rhsQ, a->rhsQf)
-                    : wadg_euler_vol_3d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->ntJ,
-                                        a->Drq, a->Dsq, a->Dtq, a->Drstq, a->VqLq, a->VfPq, a->Q,
-                                        Qf, rhsQ, a->rhsQf);
-    else
-      r = a->curved ? wadg_euler_vol_2d_curved(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ,
-                                               a->Drq, a->Dsq, a->VqLq, a->VfPq, a->Q, Qf,
-                                               rhsQ, a->rhsQf)
-                    : wadg_euler_vol_2d(a->ctx, K, a->vgeo, a->vfgeo, a->nrJ, a->nsJ, a->Drq,
-                                        a->Dsq, a->VqLq, a->VfPq, a->Q, Qf, rhsQ, a->rhsQf);
+    r = vol(a);
     cudaEventRecord(ev[1], a->stream);
-    if (!r)
-      r = a->p.dim == 3 ? wadg_euler_surf_3d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf,
-                                             a->rhsQf, rhsQ)
-                        : wadg_euler_surf_2d(a->ctx, K, a->fgeo, a->mapPq, a->VqLq, Qf,
-                                             a->rhsQf, rhsQ);
+    if (!r) r = surf(a);
     cudaEventRecord(ev[2], a->stream);
-    if (!r) {
-      if (a->p.dim == 3)
-        r = a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
-                                                    dt, rhsQ, a->resQ, a->Q, Qf)
-                      : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                             rhsQ, a->resQ, a->Q, Qf);
-      else
-        r = a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
-                                                    dt, rhsQ, a->resQ, a->Q, Qf)
-                      : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
-                                             rhsQ, a->resQ, a->Q, Qf);
-    }
+    if (!r) r = update(a, rka, rkb, dt);
     cudaEventRecord(ev[3], a->stream);
     cudaError_t e = cudaEventSynchronize(ev[3]);
     if (e != cudaSuccess && !r) r = afail(WADG_ERR_CUDA, "time_kernels", e);
