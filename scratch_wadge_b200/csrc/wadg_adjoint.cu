@@ -25,6 +25,7 @@
 #include "wadg_adjoint_kernels.cuh"
 #include "wadg_adjoint_mma.cuh"
 #include "wadg_app_impl.h"
+#include "wadg_host.h"
 
 namespace wadg_internal {
 void set_error(const std::string &msg);  // wadg_capi.cu
@@ -68,16 +69,7 @@ int ck(cudaError_t e, const char *what) {
   return e == cudaSuccess ? WADG_OK : jfail(WADG_ERR_CUDA, what, e);
 }
 
-int num_sms_adj() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+int num_sms_adj() { return wadg_internal::sm_count(); }
 
 constexpr int pickE(int target, int per) { return per >= target ? 1 : target / per; }
 
@@ -107,8 +99,8 @@ int launch_seed(const wadg_adjoint *j, cudaStream_t s, double b, double dt) {
   const wadg_app *a = j->app;
   using C = AdjMmaCfg<DIM, N, CURVED>;
   auto kern = adj_seed_mma_kernel<DIM, N, CURVED>;
-  static bool attr = false;
-  if (int r = set_smem(kern, C::smem, attr, "adjoint seed kernel smem attribute")) return r;
+  static wadg_internal::PerDevice<bool> attr;
+  if (int r = set_smem(kern, C::smem, attr.here(), "adjoint seed kernel smem attribute")) return r;
   kern<<<(a->K + C::EW - 1) / C::EW, C::threads, C::smem, s>>>(a->K, a->Jq, j->VqPqT, j->VqLqT, b,
                                                                dt, j->Qbar, j->resbar, j->rhsbar,
                                                                j->sfbar);
@@ -122,8 +114,8 @@ int launch_pairs(const wadg_adjoint *j, cudaStream_t s, const double *uq, const 
   using C = AdjPairsCfg<DIM, N, CURVED, W>;
   static_assert(C::smem <= 227 * 1024, "pair VJP kernel does not fit in shared memory");
   auto kern = adj_pairs_kernel<DIM, N, CURVED, W>;
-  static bool attr = false;
-  if (int r = set_smem(kern, C::smem, attr, "adjoint pair kernel smem attribute")) return r;
+  static wadg_internal::PerDevice<bool> attr;
+  if (int r = set_smem(kern, C::smem, attr.here(), "adjoint pair kernel smem attribute")) return r;
   const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
   const int batches = (a->K + C::E - 1) / C::E;
   const int grid = batches < num_sms_adj() * per_sm ? batches : num_sms_adj() * per_sm;
@@ -143,8 +135,8 @@ int launch_proj(const wadg_adjoint *j, cudaStream_t s, const double *Qs, double 
   using C = AdjMmaCfg<DIM, N, CURVED>;
   auto kern = seed_next ? adj_proj_mma_kernel<DIM, N, CURVED, true>
                         : adj_proj_mma_kernel<DIM, N, CURVED, false>;
-  static bool attr[2] = {false, false};
-  if (int r = set_smem(kern, C::smem, attr[seed_next], "adjoint projection kernel smem attribute"))
+  static wadg_internal::PerDevice<bool> attr[2];
+  if (int r = set_smem(kern, C::smem, attr[seed_next].here(), "adjoint projection kernel smem attribute"))
     return r;
   kern<<<(a->K + C::EW - 1) / C::EW, C::threads, C::smem, s>>>(
       a->K, a->Jq, j->VqPqT, j->VfPqT, Qs, j->vbar, j->vfbar, ra, rb, j->Qbar, j->resbar, j->phys,

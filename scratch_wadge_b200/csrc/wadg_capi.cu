@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/wadg.h"
+#include "wadg_host.h"
 #include "wadg_diag.cuh"
 #include "wadg_kernels.cuh"
 #include "wadg_surf_mma.cuh"
@@ -59,10 +60,10 @@ int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo
   constexpr int E = volE<DIM, N>();
   using C = VolCfg<DIM, N, CURVED, E>;
   auto kern = vol_kernel<DIM, N, CURVED, E>;
-  static bool attr = false;
-  if (!attr) {
+  static wadg_internal::PerDevice<bool> attr;
+  if (!attr.here()) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-    attr = true;
+    attr.here() = true;
   }
   const int grid = (K + E - 1) / E;
   kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
@@ -80,16 +81,7 @@ constexpr int volpairsW() {
   return w >= 12 ? 12 : (w < 2 ? 2 : (int)(w & ~size_t(1)));
 }
 
-int num_sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+int num_sms() { return wadg_internal::sm_count(); }
 
 // candidate CTA shapes of the pair volume kernel (warps per CTA; elements per
 // CTA = warps / 2 * 32 / lanes per element): the largest that fits in shared
@@ -108,11 +100,11 @@ int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const doubl
   using C = VolPairsCfg<DIM, N, CURVED, W>;
   static_assert(C::smem_vol <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
   auto kern = vol_pairs_kernel<DIM, N, CURVED, W>;
-  static bool attr = false;
-  if (!attr) {
+  static wadg_internal::PerDevice<bool> attr;
+  if (!attr.here()) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_vol);
     if (e != cudaSuccess) return cuda_check(e, "volume kernel smem attribute");
-    attr = true;
+    attr.here() = true;
   }
   const int per_sm = (int)((227 * 1024) / C::smem_vol) > 0 ? (int)((227 * 1024) / C::smem_vol) : 1;
   const int batches = (K + C::E - 1) / C::E;
@@ -157,11 +149,11 @@ int launch_stage(const wadg_ctx *c, int K, const double *vgeo, const double *vfg
   constexpr int W = volpairsW<DIM, N, CURVED>();
   using C = VolPairsCfg<DIM, N, CURVED, W>;
   auto kern = stage_kernel<DIM, N, CURVED, W>;
-  static bool attr = false;
-  if (!attr) {
+  static wadg_internal::PerDevice<bool> attr;
+  if (!attr.here()) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
     if (e != cudaSuccess) return cuda_check(e, "stage kernel smem attribute");
-    attr = true;
+    attr.here() = true;
   }
   const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
   const int batches = (K + C::E - 1) / C::E;
@@ -188,7 +180,8 @@ int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq
   using C = UpdMmaCfg<DIM, N, CURVED>;
   static_assert(C::smem <= 227 * 1024, "update kernel does not fit in shared memory");
   auto kern = update_mma_kernel<DIM, N, CURVED>;
-  static int per_sm = 0;
+  static wadg_internal::PerDevice<int> per_sm_dev;
+  int &per_sm = per_sm_dev.here();
   if (!per_sm) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
     if (e != cudaSuccess) return cuda_check(e, "update kernel smem attribute");
