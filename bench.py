@@ -475,6 +475,8 @@ def run_ensemble_measurement(steps=5, warmup=2):
             tuning = {str(N): {"vol_warps": b["tuning"][0],
                                "vol_ms_per_candidate": {str(w): t for w, t in b["tuning"][1].items()}}
                       for N, b in ens.bins.items()}
+            if ens.joint_tuning:  # per-bin shapes against the defaults, bins run together
+                tuning["joint"] = ens.joint_tuning
         ens.run(dt, warmup)
         ms = ens.time_run(dt, steps)
         res["fused" if fused else "three_kernels"] = ms / steps

@@ -72,23 +72,33 @@ int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo
 }
 
 // warps per CTA of the pair-scheduled volume kernel: an even count, as many
-// as fit in 227 KB of shared memory, at most 12 (register budget ~170/thread)
+// as fit in 227 KB of shared memory, at most `cap`
 template <int DIM, int N, bool CURVED>
-constexpr int volpairsW() {
+constexpr int volpairsW_fit(int cap) {
   using C = VolPairsCfg<DIM, N, CURVED, 2>;
   constexpr size_t per_warp = C::per_elem * VolTile<DIM, N>::G / C::H;
   constexpr size_t w = (227 * 1024 - C::fixed) / per_warp;
-  return w >= 12 ? 12 : (w < 2 ? 2 : (int)(w & ~size_t(1)));
+  return w >= (size_t)cap ? cap : (w < 2 ? 2 : (int)(w & ~size_t(1)));
+}
+
+// the default shape: at most 12 warps (register budget ~170 per thread)
+template <int DIM, int N, bool CURVED>
+constexpr int volpairsW() {
+  return volpairsW_fit<DIM, N, CURVED>(12);
 }
 
 int num_sms() { return wadg_internal::sm_count(); }
 
 // candidate CTA shapes of the pair volume kernel (warps per CTA; elements per
-// CTA = warps / 2 * 32 / lanes per element): the largest that fits in shared
-// memory, and two and four warps fewer
+// CTA = warps / 2 * 32 / lanes per element): the default, then two and four
+// warps fewer.  In 2D the second is 16 warps where they fit: four fields need
+// fewer registers (128 per thread), and large 2D meshes run fastest at 16,
+// small ones at 8
 template <int DIM, int N, bool CURVED>
 constexpr int volpairsW_cand(int i) {
   constexpr int W0 = volpairsW<DIM, N, CURVED>();
+  constexpr int Wbig = DIM == 2 ? volpairsW_fit<DIM, N, CURVED>(16) : W0;
+  if (i == 1 && Wbig > W0) return Wbig;
   return i == 0 ? W0 : (W0 - 2 * i >= 2 ? W0 - 2 * i : 0);
 }
 

@@ -110,14 +110,59 @@ class Ensemble:
                 tuning = app.autotune(autotune_dt)
             app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
             self.bins[N] = dict(idx=idx, geo=geo, state=st, offs=offs, app=app, tuning=tuning)
+        self.h = None
+        self.joint_tuning = None
+        if autotune_dt is not None:
+            self._tune_jointly(autotune_dt)
+        self.h = self._create()
+        self.K = sum(g.K for g, _ in self.parts)
+        self.dofs = sum(g.K * g.ops.Np for g, _ in self.parts)
+
+    def _create(self):
         apps = (ctypes.c_void_p * len(self.bins))(*[b["app"].h.value for b in self.bins.values()])
         h = ctypes.c_void_p()
         L = capi.lib()
         L.wadg_ensemble_create.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
         capi.check(L.wadg_ensemble_create(len(self.bins), apps, ctypes.byref(h)), "ensemble_create")
-        self.h = h
-        self.K = sum(g.K for g, _ in self.parts)
-        self.dofs = sum(g.K * g.ops.Np for g, _ in self.parts)
+        return h
+
+    def _set_shapes(self, shapes):
+        L = capi.lib()
+        for N, b in self.bins.items():
+            ctx = ctypes.c_void_p(L.wadg_app_ctx(b["app"].h))
+            capi.check(L.wadg_ctx_set_vol_warps(ctx, 1, shapes[N]), "set_vol_warps")
+
+    def _tune_jointly(self, dt, steps=3):
+        """Each bin's shape was tuned alone, but the bins run concurrently:
+        keep the per-bin choices only if the whole batched step is faster
+        with them than with every bin at its default shape."""
+        tuned = {N: b["tuning"][0] for N, b in self.bins.items()}
+        default = {N: 0 for N in self.bins}
+        if all(tuned[N] == self._default_shape(N) for N in self.bins):
+            return
+        times = {}
+        L = capi.lib()
+        for name, shapes in (("tuned", tuned), ("default", default)):
+            self._set_shapes(shapes)
+            h = self._create()
+            self.h = h
+            try:
+                self.run(dt, 1)
+                times[name] = self.time_run(dt, steps) / steps
+            finally:
+                L.wadg_ensemble_destroy(h)
+                self.h = None
+        best = "tuned" if times["tuned"] <= times["default"] else "default"
+        self._set_shapes(tuned if best == "tuned" else default)
+        self.joint_tuning = dict(ms_per_step=times, kept=best)
+        self.reset()
+
+    def _default_shape(self, N):
+        L = capi.lib()
+        ctx = ctypes.c_void_p(L.wadg_app_ctx(self.bins[N]["app"].h))
+        cand = (ctypes.c_int * 3)()
+        L.wadg_vol_warps_candidates(ctx, 1, cand)
+        return int(cand[0])
 
     def close(self):
         if getattr(self, "h", None):

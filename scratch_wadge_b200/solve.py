@@ -73,6 +73,9 @@ def main(argv=None):
                     help="dt = CFL hmin / C_N exactly as the reference (by default dt is also divided by "
                          "the initial maximum wave speed, which the Taylor-Green state needs)")
     ap.add_argument("--fused", action="store_true", help="the fused one-launch stage kernel")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default CTA shape of the volume kernel (by default a few stages "
+                         "are timed per candidate shape and the fastest is kept)")
     ap.add_argument("--time-kernels", type=int, default=0, metavar="STAGES",
                     help="also time the volume, surface and update kernels over this many stages")
     ap.add_argument("--datadir", default=None, help="write the mesh as MFEM here (app.output.datadir)")
@@ -98,6 +101,10 @@ def main(argv=None):
     dt, nsteps = IC.time_step(geo, args.cfl, args.N, args.final_time, args.steps, wave_speed=wave)
     app.set_fused(args.fused)
     S0 = IC.entropy(geo, solver.Q0, args.gamma)
+    warps = None
+    if not args.no_autotune:
+        warps, _ = app.autotune(dt, 5)
+        solver.reset()
 
     kernels = None
     if args.time_kernels:
@@ -114,6 +121,8 @@ def main(argv=None):
                finite=bool(np.isfinite(Q).all()))
     if kernels:
         out["kernel_ms"] = kernels
+    if warps is not None:
+        out["vol_warps"] = warps
     if kind in ("vortex", "density_wave", "constant"):
         out["l2_error"] = IC.l2_error(geo, Q, IC.exact_state(geo, kind, dt * nsteps, args.gamma))
     if args.datadir:
