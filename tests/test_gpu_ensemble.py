@@ -37,6 +37,35 @@ def test_batched_equals_single(cuda, small, fused):
     single.close()
 
 
+def test_autotuned_ensemble(cuda, small):
+    """Per-bin shape tuning, then the joint check of the batched step: the
+    shapes kept are compiled candidates, the tuned ensemble starts from the
+    initial state, and its results equal the plain path's."""
+    import ctypes
+    from scratch_wadge_b200 import capi
+    inst, parts, dt = small
+    ens = EN.Ensemble(inst, parts, autotune_dt=dt)
+    L = capi.lib()
+    for N, b in ens.bins.items():
+        ctx = ctypes.c_void_p(L.wadg_app_ctx(b["app"].h))
+        cand = (ctypes.c_int * 3)()
+        n = L.wadg_vol_warps_candidates(ctx, 1, cand)
+        w = L.wadg_ctx_get_vol_warps(ctx)
+        assert w == 0 or w in list(cand[:n]), (N, w)
+        assert b["tuning"][0] in list(cand[:n])
+    if ens.joint_tuning is not None:
+        assert ens.joint_tuning["kept"] in ("tuned", "default")
+    single = EN.SingleInstances(inst, parts)
+    ens.run(dt, 2)
+    single.run(dt, 2)
+    for j in range(len(inst)):
+        a = ens.instance_state(j)
+        b = single.apps[j].get_state()
+        assert rel(a["Q"], b["Q"]) < RTOL, j
+    ens.close()
+    single.close()
+
+
 def test_batched_matches_oracle(cuda, small):
     inst, parts, dt = small
     ens = EN.Ensemble(inst, parts)
