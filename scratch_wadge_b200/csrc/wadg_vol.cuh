@@ -169,11 +169,12 @@ struct VolPairs {
       st[(DIM + 1) * NN + n] = s.beta;
       st[(DIM + 2) * NN + n] = s.lrho;
       st[(DIM + 3) * NN + n] = s.lbeta;
-      if (CURVED) {
+      if (CURVED) {  // geometric factors stored halved: a pair's average
+                     // (G_i + G_j)/2 is then one addition, with the same bits
 #pragma unroll
         for (int c = 0; c < NG; ++c)
-          st[(NS + c) * NN + n] = (n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
-                                           : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
+          st[(NS + c) * NN + n] = 0.5 * ((n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
+                                                  : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)]);
       }
     }
     for (int t = t0; t < ne * SA; t += ts) sAcc[e0 * SA + t] = 0.0;
@@ -246,7 +247,7 @@ struct VolPairs {
           double v = 0.0;
 #pragma unroll
           for (int a = 0; a < DIM; ++a) {
-            const double gad = CURVED ? 0.5 * (st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + j])
+            const double gad = CURVED ? st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + j]
                                       : Ge[a * DIM + d];
             v = fma(gad, rr[a], v);
           }
@@ -284,7 +285,7 @@ struct VolPairs {
             double v = 0.0;
 #pragma unroll
             for (int a = 0; a < DIM; ++a)
-              v = fma(0.5 * (st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + Nq + f]),
+              v = fma(st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + Nq + f],
                       sNr[fc * DIM + a], v);
             nv[d] = v;
           }
