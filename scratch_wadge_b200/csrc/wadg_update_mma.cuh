@@ -57,10 +57,13 @@ struct UpdMmaCfg {
   static constexpr int WARPS = MQ < 2 ? 2 : (MQ > 6 ? 6 : MQ);
   static constexpr int threads = 32 * WARPS;
   static constexpr size_t smem = sizeof(double) * 2 * BUF;
-  // register cap from the launch bounds: 5 resident CTAs per SM measured best
-  // (3D N=3 affine: 0.065 ms vs 0.067 uncapped and 0.065 at 7; the
-  // latency of the per-group chain wants warps more than registers)
-  static constexpr int min_ctas = 5;
+  // register cap from the launch bounds.  Up to 3 warps per CTA, 5 resident
+  // CTAs per SM measured best (3D N=3 affine: 0.065 ms vs 0.067 uncapped and
+  // 0.065 at 7; the latency of the per-group chain wants warps more than
+  // registers).  At 6 warps (N=4 in 3D), 5 CTAs cap the registers at 64 and
+  // spill: 3 CTAs measured best (curved N=4: 0.0885 ms vs 0.0965 at 5,
+  // 0.100 at 2, 0.091 at 4)
+  static constexpr int min_ctas = WARPS >= 6 ? 3 : 5;
 };
 
 // A fragments of rows [8 mt, 8 mt + 8) of an operator stored column-major
