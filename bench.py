@@ -513,6 +513,18 @@ def fp64_peak(stream):
     return best
 
 
+def launch_ranks(n, argv):
+    """Re-run this script as n ranks on this node (torch.distributed.run on
+    127.0.0.1, a free port); returns the launcher's exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + argv
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -530,6 +542,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.gpus > 1 and ws == 1 and "RANK" not in os.environ:
+        # not under a launcher: start one rank per GPU here
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
+    if ws != args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} but the launcher started {ws} rank(s) "
+                 f"(WORLD_SIZE={ws}); run it under torchrun with --nproc-per-node {args.gpus}")
     if args.impl == "reference":
         run_reference(args)
     else:

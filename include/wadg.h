@@ -68,6 +68,24 @@ int wadg_ctx_set_stream(wadg_ctx *ctx, void *stream);
 int wadg_vol_warps_candidates(const wadg_ctx *ctx, int curved, int *out);
 int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps);
 int wadg_ctx_get_vol_warps(const wadg_ctx *ctx);
+/* Launch shape of one kernel for K elements, the numbers its entry point
+ * uses: elements per batch (one CTA pass) and CTAs launched.  The volume,
+ * update and fused stage kernels are persistent: CTA b takes batches b,
+ * b + grid, b + 2 grid, ..., so K > elems * grid makes CTAs run several
+ * batches, and K not a multiple of elems leaves a partial last batch.  The
+ * volume kernel's shape follows the context's wadg_ctx_set_vol_warps.  For
+ * tests and tuning; no counterpart in the reference (OCCA launches one
+ * work-group per Kblk elements, euler.c:2879-2950). */
+enum
+{
+  WADG_KERNEL_VOL = 0,
+  WADG_KERNEL_SURF = 1,
+  WADG_KERNEL_UPDATE = 2,
+  WADG_KERNEL_STAGE = 3,
+  WADG_KERNEL_ADJ_PAIRS = 4 /* the adjoint's pair VJP kernel (persistent) */
+};
+int wadg_kernel_shape(const wadg_ctx *ctx, int kernel, int curved, int K, int *elems_per_batch,
+                      int *grid);
 const char *wadg_last_error(void);
 /* degrees compiled for `dim`, as a bit mask (bit N set = degree N) */
 int wadg_supported_degrees(int dim);
@@ -210,6 +228,18 @@ int wadg_match_faces(const wadg_geo_ops *ops, int K, const double *xa,
 int wadg_halo_pack(wadg_ctx *ctx, int n, const uint32_t *src, const double *Qf,
                    size_t nQf, double *buf);
 
+/* Failure detection.  Scans the conserved state Q [K][Nfields][Nq] for
+ * non-physical nodes: a field that is NaN or infinite, rho <= 0, or a
+ * pressure (gamma-1)(E - |m|^2/(2 rho)) <= 0.  `work` is a caller-owned device
+ * buffer of 2 ints.  Synchronous (waits for the context's stream).  Returns
+ * WADG_OK when every node is physical; otherwise WADG_ERR_STATE, with
+ * *nbad = the number of bad nodes, *first = the smallest bad node index
+ * k*Nq + i, and wadg_last_error() naming it (nbad and first may be NULL).
+ * The reference has no such check: a bad state runs on into NaNs, and its
+ * only failure path is an abort (ASD_ABORT, asd.h:77-79); this call returns a
+ * status instead. */
+int wadg_check_state(wadg_ctx *ctx, int K, const double *Q, int *work, int *nbad, int *first);
+
 /* ------------------------------------------------------------ mesh I/O
  * The host driver's mesh files.  wadg_mesh_read_gmsh reads ASCII gmsh 2.x as
  * host_mesh_read_msh does (euler.c:556-833): the nodes; the elements of type
@@ -323,6 +353,13 @@ int wadg_rk_step(wadg_app *app, double rka, double rkb, double dt);
  * use_graph != 0 one time step (15 launches) is captured once as a CUDA graph
  * and replayed. Asynchronous. */
 int wadg_rk_run(wadg_app *app, double dt, int nsteps, int use_graph);
+/* Failure detection in the time loop: with nsteps > 0, wadg_rk_run checks
+ * the state (wadg_check_state) every nsteps steps and after the last one,
+ * and stops with WADG_ERR_STATE at the first check that finds a bad node
+ * (the message names the step); each check synchronises the stream.  0 (the
+ * default) never checks.  wadg_app_check_state checks the app's Q now. */
+int wadg_app_set_check_every(wadg_app *app, int nsteps);
+int wadg_app_check_state(wadg_app *app, int *nbad, int *first);
 /* The whole user-level solve with HOST buffers: copy the stage-0 state in,
  * run nsteps, copy Q out (and the other state arrays if non-NULL).
  * Synchronous. */
@@ -331,11 +368,11 @@ int wadg_app_solve_host(wadg_app *app, const double *Q0, const double *rhsQ0,
                         int nsteps, double *Q, double *rhsQ, double *Qf,
                         double *resQ);
 /* The entropy projection of the app's Q into the traces the next stage
- * reads (rhsQ = U(VqPq v), Qf = U(VfPq v), v = V(Q); curved: the
- * weight-adjusted projection of the update kernel), and resQ = 0: the
+ * reads (rhsQ = U(VqPq v), Qf = U(VfPq v), v = V(Q)), and resQ = 0: the
  * stage-0 state the reference's driver builds on the host
- * (euler.c:3958-4133; its curved path projects with VqPq alone).
- * Asynchronous. */
+ * (euler.c:3958-4133).  As there, curved meshes are projected with VqPq
+ * alone too (the weight-adjusted projection is the curved update kernel's,
+ * applied from the first stage's update on).  Asynchronous. */
 int wadg_app_project(wadg_app *app);
 /* The user-level solve from the conserved state alone: copy Q0 in, project
  * (wadg_app_project), run nsteps, copy Q out.  Synchronous. */
@@ -407,9 +444,12 @@ int wadg_ensemble_time_run(wadg_ensemble *ens, double dt, int nsteps, float *ms)
  * WADG_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB), resident on every GPU that
  * loads the library until the process exits.  Limit: K * Nfq*Nfaces *
  * Nfields must not exceed it (3D N=3: K <= 8738); larger K is rejected with
- * WADG_ERR_INVALID.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture.  All calls share
- * the array: calls that overlap on the GPU race, so serialise them. */
+ * WADG_ERR_INVALID.  Each call outside a stream capture looks up the
+ * array's device address on the current device (so a context made again
+ * after cudaDeviceReset is followed); a call during a capture reuses the
+ * address the last call on that device found, so make the first call on a
+ * device before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so serialise them. */
 #define WADG_NOALLOC_SCRATCH_DOUBLES (2 * 1024 * 1024)
 int wadg_rk_stage_noalloc(wadg_ctx *ctx, int K, int curved, const double *vgeo,
                           const double *vfgeo, const double *fgeo,

@@ -29,7 +29,10 @@ import sys
 import tarfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DIR = os.environ.get("WADG_REFERENCE_DIR", "/root/reference")
+# the reference checkout: $WADG_REFERENCE_DIR, else a directory named
+# "reference" beside the repository's own (absent on GPU hosts)
+REF_DIR = os.environ.get("WADG_REFERENCE_DIR",
+                         os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 OUT_REF = os.path.join(HERE, "_ref")
 OUT_PORT = os.path.join(HERE, "_build")
 

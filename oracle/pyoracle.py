@@ -6,7 +6,8 @@
 
 Both expose the same three calls with the reference's argument meaning:
     vol(geo, Qf, rhsQ, rhsQf)      rhsQ in: u(VqPq v), out: volume RHS
-    surf(geo, Qf, rhsQf, rhsQ)     rhsQ += lift of the surface flux
+    surf(geo, Qf, rhsQf, rhsQ)     rhsQ += lift of the surface flux (over the
+                                   elements of rhsQ; Qf may hold more)
     update(geo, fa, fb, dt, rhsQ, resQ, Q, Qf)
 All arrays are float64 numpy arrays in the kernel layouts; they are updated in
 place.  ``stage`` / ``step`` chain them like rk_step / rk_run (euler.c:3610-3699).
@@ -121,7 +122,7 @@ class Port(_Base):
                                    _p(self.VqLq), _p(self.VfPq), _p(Qf), _p(rhsQ), _p(rhsQf))
 
     def surf(self, geo, Qf, rhsQf, rhsQ):
-        K = Qf.shape[0]
+        K = rhsQ.shape[0]  # Qf may be longer: neighbour traces are gathered from all of it
         fn = self.L.wadg_ref_surf_3d if self.ops.dim == 3 else self.L.wadg_ref_surf_2d
         fn(ctypes.byref(self.d), K, _p(geo.fgeo), _u(geo.mapPq), _p(self.VqLq), _p(Qf), _p(rhsQf), _p(rhsQ))
 
@@ -181,7 +182,7 @@ class Reference(_Base):
                       _p(Qdummy), _p(Qf), _p(rhsQ), _p(rhsQf))
 
     def surf(self, geo, Qf, rhsQf, rhsQ):
-        K = Qf.shape[0]
+        K = rhsQ.shape[0]  # Qf may be longer: neighbour traces are gathered from all of it
         self._surf(K, _p(geo.fgeo), _u(geo.mapPq), _p(self.VqLq), _p(Qf), _p(rhsQf), _p(rhsQ))
 
     def update(self, geo, fa, fb, fdt, rhsQ, resQ, Q, Qf):

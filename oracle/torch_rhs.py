@@ -27,11 +27,13 @@ import torch
 
 
 class TorchRHS:
-    def __init__(self, geo, curved, gamma=1.4, tau=1.0):
+    def __init__(self, geo, curved, gamma=1.4, tau=1.0, device=None):
+        """device: where the restated map's tensors live (CPU by default; a
+        CUDA device runs the check at large K through torch's own kernels)"""
         ops = geo.ops
         self.dim, self.curved, self.gamma = ops.dim, bool(curved), gamma
         self.tau = tau if ops.dim == 3 else 1.0
-        t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64)
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=device)
         self.K, self.Nq, self.NF, self.Nfq = geo.K, ops.Nq, ops.NfqNf, ops.Nfq
         self.Nf = ops.dim + 2
         self.D = [t(ops.Drq), t(ops.Dsq)] + ([t(ops.Dtq)] if ops.dim == 3 else [])
@@ -47,7 +49,8 @@ class TorchRHS:
         self.Jq = t(geo.Jq)                                                # [K, Nq]
         mp = np.asarray(geo.mapPq, dtype=np.int64).reshape(self.K, self.NF)
         blk = self.NF * self.Nf
-        self.mapK, self.mapJ = torch.as_tensor(mp // blk), torch.as_tensor(mp % blk)
+        self.mapK = torch.as_tensor(mp // blk, device=device)
+        self.mapJ = torch.as_tensor(mp % blk, device=device)
         # the reference's float thresholds 1.fe-4 / 1.fe-3, as doubles
         self.thr = float(np.float32(1e-4)) if d == 3 else float(np.float32(1e-3))
 

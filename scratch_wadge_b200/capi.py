@@ -32,8 +32,14 @@ _V = ctypes.c_void_p
 _lib = None
 
 
+# status codes (include/wadg.h)
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_STATE = 0, 1, 2, 3, 4
+
+
 class WadgError(RuntimeError):
-    pass
+    def __init__(self, msg, code=None):
+        super().__init__(msg)
+        self.code = code
 
 
 class Params(ctypes.Structure):
@@ -103,6 +109,10 @@ def lib():
         L.wadg_vol_warps_candidates.argtypes = [v, i, ctypes.POINTER(ctypes.c_int)]
         L.wadg_ctx_set_vol_warps.argtypes = [v, i, i]
         L.wadg_ctx_get_vol_warps.argtypes = [v]
+        L.wadg_check_state.argtypes = [v, i, v, v, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.wadg_app_check_state.argtypes = [v, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.wadg_app_set_check_every.argtypes = [v, i]
+        L.wadg_kernel_shape.argtypes = [v, i, i, i, ctypes.POINTER(i), ctypes.POINTER(i)]
         L.wadg_app_autotune.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_float)]
         L.wadg_adjoint_create.argtypes = [v, i, i, ctypes.POINTER(ctypes.c_void_p)]
@@ -131,7 +141,7 @@ def lib():
 def check(code: int, what: str = ""):
     if code != 0:
         msg = lib().wadg_last_error().decode()
-        raise WadgError(f"{what} failed ({code}): {msg}")
+        raise WadgError(f"{what} failed ({code}): {msg}", code)
 
 
 def params_for(ops: R.RefOps, gamma=1.4, tau=1.0, stream=None) -> Params:
@@ -203,6 +213,36 @@ class Context:
     def element_entropy(self, K, Jq, wq, Q, S):
         """per-element entropy integral sum_i w J (-rho s)"""
         check(lib().wadg_element_entropy(self.h, K, Jq, wq, Q, S), "element_entropy")
+
+    def check_state(self, K, Q, work):
+        """Failure detection (wadg_check_state): (status, bad nodes, first bad
+        node index k*Nq + i or -1); status 0 or WADG_ERR_STATE (4)"""
+        nbad, first = ctypes.c_int(), ctypes.c_int()
+        r = lib().wadg_check_state(self.h, K, Q, work, ctypes.byref(nbad), ctypes.byref(first))
+        if r not in (0, ERR_STATE):
+            check(r, "check_state")
+        return r, nbad.value, first.value
+
+    KERNELS = {"vol": 0, "surf": 1, "update": 2, "stage": 3, "adj_pairs": 4}
+
+    def shape(self, kernel, curved, K):
+        """(elements per batch, CTAs launched) of `kernel` for K elements
+        (wadg_kernel_shape); persistent CTAs run several batches when
+        K > elements * CTAs"""
+        E, g = ctypes.c_int(), ctypes.c_int()
+        check(lib().wadg_kernel_shape(self.h, self.KERNELS[kernel], int(curved), K, ctypes.byref(E),
+                                      ctypes.byref(g)), "kernel_shape")
+        return E.value, g.value
+
+    def set_vol_warps(self, curved, warps):
+        check(lib().wadg_ctx_set_vol_warps(self.h, int(curved), warps), "set_vol_warps")
+
+    def vol_warps_candidates(self, curved):
+        c = (ctypes.c_int * 3)()
+        n = lib().wadg_vol_warps_candidates(self.h, int(curved), c)
+        if n < 1:
+            raise WadgError(lib().wadg_last_error().decode())
+        return [c[k] for k in range(n)]
 
     def update(self, curved, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf):
         L = lib()
@@ -277,6 +317,19 @@ class App:
 
     def sync(self):
         check(lib().wadg_app_sync(self.h), "sync")
+
+    def check_state(self):
+        """(status, bad nodes, first bad node) of the app's Q (wadg_app_check_state)"""
+        nbad, first = ctypes.c_int(), ctypes.c_int()
+        r = lib().wadg_app_check_state(self.h, ctypes.byref(nbad), ctypes.byref(first))
+        if r not in (0, ERR_STATE):
+            check(r, "check_state")
+        return r, nbad.value, first.value
+
+    def set_check_every(self, nsteps):
+        """wadg_rk_run checks the state every nsteps steps (0 = never) and
+        raises WadgError (code WADG_ERR_STATE) at the first bad one"""
+        check(lib().wadg_app_set_check_every(self.h, nsteps), "set_check_every")
 
     def solve_host(self, Q0, rhsQ0, Qf0, dt, nsteps, resQ0=None, out=None):
         """User-level solve with host buffers (H2D, nsteps, D2H of Q)."""

@@ -107,6 +107,15 @@ int launch_seed(const wadg_adjoint *j, cudaStream_t s, double b, double dt) {
   return ck(cudaGetLastError(), "adjoint seed kernel");
 }
 
+// CTAs of the persistent pair VJP kernel over K elements (batches of C::E)
+template <int DIM, int N, bool CURVED>
+int pairs_grid(int K) {
+  using C = AdjPairsCfg<DIM, N, CURVED, adjW<DIM, N, CURVED>()>;
+  const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
+  const int batches = (K + C::E - 1) / C::E;
+  return batches < num_sms_adj() * per_sm ? batches : num_sms_adj() * per_sm;
+}
+
 template <int DIM, int N, bool CURVED>
 int launch_pairs(const wadg_adjoint *j, cudaStream_t s, const double *uq, const double *uf) {
   const wadg_app *a = j->app;
@@ -116,9 +125,7 @@ int launch_pairs(const wadg_adjoint *j, cudaStream_t s, const double *uq, const 
   auto kern = adj_pairs_kernel<DIM, N, CURVED, W>;
   static wadg_internal::PerDevice<bool> attr;
   if (int r = set_smem(kern, C::smem, attr.here(), "adjoint pair kernel smem attribute")) return r;
-  const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
-  const int batches = (a->K + C::E - 1) / C::E;
-  const int grid = batches < num_sms_adj() * per_sm ? batches : num_sms_adj() * per_sm;
+  const int grid = pairs_grid<DIM, N, CURVED>(a->K);
   kern<<<grid, C::threads, C::smem, s>>>(a->K, a->vgeo, a->vfgeo, a->fgeo, a->mapPq, a->nrJ,
                                                   a->nsJ, a->ntJ, a->Drq, a->Dsq, a->Dtq, a->VqLq,
                                                   a->VfPq, uq, uf, j->rhsbar, j->sfbar, j->vbar,
@@ -177,6 +184,27 @@ int stage_adjoint(const wadg_adjoint *j, cudaStream_t s, const StageStep &st) {
 #undef WADG_ADJ_CASE
   return jfail(WADG_ERR_UNSUPPORTED, "degree not compiled");
 }
+
+}  // namespace
+
+namespace wadg_internal {
+// launch shape of the pair VJP kernel (wadg_kernel_shape)
+int adj_pairs_shape(int dim, int N, bool curved, int K, int *E, int *grid) {
+#define WADG_ADJ_SHAPE(D_, N_)                                                                     \
+  if (dim == D_ && N == N_) {                                                                      \
+    *E = curved ? AdjPairsCfg<D_, N_, true, adjW<D_, N_, true>()>::E                               \
+                : AdjPairsCfg<D_, N_, false, adjW<D_, N_, false>()>::E;                            \
+    *grid = curved ? pairs_grid<D_, N_, true>(K) : pairs_grid<D_, N_, false>(K);                   \
+    return WADG_OK;                                                                                \
+  }
+  WADG_ADJ_SHAPE(2, 1) WADG_ADJ_SHAPE(2, 2) WADG_ADJ_SHAPE(2, 3) WADG_ADJ_SHAPE(2, 4)
+  WADG_ADJ_SHAPE(3, 1) WADG_ADJ_SHAPE(3, 2) WADG_ADJ_SHAPE(3, 3) WADG_ADJ_SHAPE(3, 4)
+#undef WADG_ADJ_SHAPE
+  return jfail(WADG_ERR_UNSUPPORTED, "degree not compiled");
+}
+}  // namespace wadg_internal
+
+namespace {
 
 // the update kernel with a zero RHS and zero coefficients: Q unchanged, res = 0,
 // u~ and uf~ = the entropy projection of Q (the traces the next stage reads)

@@ -53,6 +53,7 @@ void free_all(wadg_app *a) {
   for (double *b : bufs)
     if (b) cudaFree(b);
   if (a->mapPq) cudaFree(a->mapPq);
+  if (a->check_work) cudaFree(a->check_work);
   for (auto &g : a->graph)
     if (g) cudaGraphExecDestroy(g);
   if (a->ctx) wadg_ctx_destroy(a->ctx);
@@ -85,15 +86,17 @@ int surf(wadg_app *a) {
                                             a->rhsQf, rhsQ);
 }
 
-int update(wadg_app *a, double rka, double rkb, double dt) {
+// wadg: the curved update (weight-adjusted inverse mass and projection) on
+// a curved app; false runs the affine update (used for the stage-0 projection)
+int update(wadg_app *a, double rka, double rkb, double dt, bool wadg) {
   const int K = a->K;
   double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
   if (a->p.dim == 3)
-    return a->curved ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
+    return wadg ? wadg_euler_update_3d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb,
                                                    dt, rhsQ, a->resQ, a->Q, Qf)
                      : wadg_euler_update_3d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
                                             rhsQ, a->resQ, a->Q, Qf);
-  return a->curved ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
+  return wadg ? wadg_euler_update_2d_curved(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt,
                                                  rhsQ, a->resQ, a->Q, Qf)
                    : wadg_euler_update_2d(a->ctx, K, a->Jq, a->VqPq, a->VfPq, rka, rkb, dt, rhsQ,
                                           a->resQ, a->Q, Qf);
@@ -102,7 +105,7 @@ int update(wadg_app *a, double rka, double rkb, double dt) {
 int stage3(wadg_app *a, double rka, double rkb, double dt) {
   int r = vol(a);
   if (!r) r = surf(a);
-  if (!r) r = update(a, rka, rkb, dt);
+  if (!r) r = update(a, rka, rkb, dt, a->curved);
   return r;
 }
 
@@ -204,6 +207,11 @@ int wadg_app_create(const wadg_params *p, int K, int curved, const wadg_host_dat
     delete a;
     return afail(WADG_ERR_INVALID, "missing host array");
   }
+  if ((unsigned long long)K * a->NfqNf * a->Nf > 0xffffffffULL) {
+    free_all(a);
+    delete a;
+    return afail(WADG_ERR_INVALID, "K * NfqNf * Nfields exceeds the 32-bit range of mapPq");
+  }
   if (!valid_map(h->mapPq, K, a->NfqNf, a->Nf)) {
     free_all(a);
     delete a;
@@ -230,7 +238,8 @@ int wadg_app_create(const wadg_params *p, int K, int curved, const wadg_host_dat
       (r = upload(&a->uf[1], (const double *)nullptr, K * NfqNf * Nf, s)) ||
       (r = upload(&a->resQ, (const double *)nullptr, K * Nq * Nf, s)) ||
       (r = upload(&a->uf[0], (const double *)nullptr, K * NfqNf * Nf, s)) ||
-      (r = upload(&a->rhsQf, (const double *)nullptr, K * NfqNf * Nf, s))) {
+      (r = upload(&a->rhsQf, (const double *)nullptr, K * NfqNf * Nf, s)) ||
+      (r = upload(&a->check_work, (const int *)nullptr, 2, s))) {
     free_all(a);
     delete a;
     return r;
@@ -295,25 +304,45 @@ int wadg_rk_step(wadg_app *a, double rka, double rkb, double dt) {
   return stage(a, rka, rkb, dt);
 }
 
+// the state check of wadg_rk_run after `steps` steps
+int check_after(wadg_app *a, int steps) {
+  int nbad = 0;
+  const int r = wadg_check_state(a->ctx, a->K, a->Q, a->check_work, &nbad, nullptr);
+  if (r != WADG_ERR_STATE) return r;
+  std::string m = "after step " + std::to_string(steps) + ": " + wadg_last_error();
+  wadg_internal::set_error(m);
+  return r;
+}
+
 int wadg_rk_run(wadg_app *a, double dt, int nsteps, int use_graph) {
   if (!a || nsteps < 0) return afail(WADG_ERR_INVALID, "invalid argument");
-  if (use_graph) {
-    for (int t = 0; t < nsteps; ++t) {
+  for (int t = 0; t < nsteps; ++t) {
+    if (use_graph) {
       const int p = a->cur;
       int r = capture_step(a, dt);
       if (r) return r;
       cudaError_t e = cudaGraphLaunch(a->graph[p], a->stream);
       if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaGraphLaunch", e);
       if (a->fused) a->cur = 1 - p;  // 5 stages flip the parity once
+    } else {
+      for (int s = 0; s < 5; ++s)
+        if (int r = stage(a, RK4A[s], RK4B[s], dt)) return r;
     }
-    return WADG_OK;
+    if (a->check_every > 0 && ((t + 1) % a->check_every == 0 || t + 1 == nsteps))
+      if (int r = check_after(a, t + 1)) return r;
   }
-  for (int t = 0; t < nsteps; ++t)
-    for (int s = 0; s < 5; ++s) {
-      int r = stage(a, RK4A[s], RK4B[s], dt);
-      if (r) return r;
-    }
   return WADG_OK;
+}
+
+int wadg_app_set_check_every(wadg_app *a, int nsteps) {
+  if (!a || nsteps < 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  a->check_every = nsteps;
+  return WADG_OK;
+}
+
+int wadg_app_check_state(wadg_app *a, int *nbad, int *first) {
+  if (!a) return afail(WADG_ERR_INVALID, "null app");
+  return wadg_check_state(a->ctx, a->K, a->Q, a->check_work, nbad, first);
 }
 
 int wadg_app_set_fused(wadg_app *a, int fused) {
@@ -340,13 +369,16 @@ int wadg_app_solve_host(wadg_app *a, const double *Q0, const double *rhsQ0, cons
 int wadg_app_project(wadg_app *a) {
   if (!a) return afail(WADG_ERR_INVALID, "null app");
   // the update kernel with a zero RHS and zero coefficients: Q unchanged,
-  // resQ = 0, the traces = the entropy projection of Q
+  // resQ = 0, the traces = the entropy projection of Q.  The affine update
+  // on curved meshes too: the reference's host builds the stage-0 traces with
+  // VqPq alone (euler.c:3958-4133), not with the weight-adjusted projection
+  // its curved update kernel applies in every later stage
   const size_t nvb = (size_t)a->K * a->Nq * a->Nf * sizeof(double);
   cudaError_t e;
   if ((e = cudaMemsetAsync(a->uq[a->cur], 0, nvb, a->stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(a->resQ, 0, nvb, a->stream)) != cudaSuccess)
     return afail(WADG_ERR_CUDA, "memset", e);
-  return update(a, 0.0, 0.0, 0.0);
+  return update(a, 0.0, 0.0, 0.0, false);
 }
 
 int wadg_app_solve_host_q(wadg_app *a, const double *Q0, double dt, int nsteps, double *Q) {
@@ -416,7 +448,7 @@ int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
     cudaEventRecord(ev[1], a->stream);
     if (!r) r = surf(a);
     cudaEventRecord(ev[2], a->stream);
-    if (!r) r = update(a, rka, rkb, dt);
+    if (!r) r = update(a, rka, rkb, dt, a->curved);
     cudaEventRecord(ev[3], a->stream);
     cudaError_t e = cudaEventSynchronize(ev[3]);
     if (e != cudaSuccess && !r) r = afail(WADG_ERR_CUDA, "time_kernels", e);

@@ -39,6 +39,10 @@ struct wadg_app {
   int fused = 0;
   // graphs of one time step, one per starting buffer parity (fused path)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // failure detection: device work words of wadg_check_state, and how often
+  // wadg_rk_run checks the state (every `check_every` steps; 0 = never)
+  int *check_work = nullptr;
+  int check_every = 0;
   double graph_dt[2] = {0.0, 0.0};
   int graph_fused[2] = {-1, -1};
 };

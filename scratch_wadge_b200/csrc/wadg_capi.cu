@@ -13,7 +13,6 @@
 #include "../../include/wadg.h"
 #include "wadg_host.h"
 #include "wadg_diag.cuh"
-#include "wadg_kernels.cuh"
 #include "wadg_surf_mma.cuh"
 #include "wadg_update_mma.cuh"
 #include "wadg_vol.cuh"
@@ -48,29 +47,6 @@ int cuda_check(cudaError_t e, const char *what) {
 
 int after_launch(const char *name) { return cuda_check(cudaGetLastError(), name); }
 
-constexpr int pickE(int target, int per) { return per >= target ? 1 : target / per; }
-
-template <int DIM, int N> constexpr int volE() { return pickE(320, Elem<DIM, N>::NN); }
-
-template <int DIM, int N, bool CURVED>
-int launch_vol(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
-               const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
-               const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
-               const double *Qf, double *rhsQ, double *rhsQf) {
-  constexpr int E = volE<DIM, N>();
-  using C = VolCfg<DIM, N, CURVED, E>;
-  auto kern = vol_kernel<DIM, N, CURVED, E>;
-  static wadg_internal::PerDevice<bool> attr;
-  if (!attr.here()) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-    attr.here() = true;
-  }
-  const int grid = (K + E - 1) / E;
-  kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
-                                                   VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
-  return after_launch("vol kernel");
-}
-
 // warps per CTA of the pair-scheduled volume kernel: an even count, as many
 // as fit in 227 KB of shared memory, at most `cap`
 template <int DIM, int N, bool CURVED>
@@ -88,6 +64,15 @@ constexpr int volpairsW() {
 }
 
 int num_sms() { return wadg_internal::sm_count(); }
+
+// CTAs of a persistent kernel over K elements in batches of E: one per batch,
+// at most as many as are resident at once (shared memory per CTA `smem`); CTA
+// b takes batches b, b + grid, b + 2 grid, ...
+int persistent_grid(int K, int E, size_t smem) {
+  const int per_sm = (int)((227 * 1024) / smem) > 0 ? (int)((227 * 1024) / smem) : 1;
+  const int batches = (K + E - 1) / E;
+  return batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
+}
 
 // candidate CTA shapes of the pair volume kernel (warps per CTA; elements per
 // CTA = warps / 2 * 32 / lanes per element): the default, then two and four
@@ -116,9 +101,7 @@ int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const doubl
     if (e != cudaSuccess) return cuda_check(e, "volume kernel smem attribute");
     attr.here() = true;
   }
-  const int per_sm = (int)((227 * 1024) / C::smem_vol) > 0 ? (int)((227 * 1024) / C::smem_vol) : 1;
-  const int batches = (K + C::E - 1) / C::E;
-  const int grid = batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
+  const int grid = persistent_grid(K, C::E, C::smem_vol);
   kern<<<grid, C::threads, C::smem_vol, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
                                                       VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
   return after_launch("volume kernel");
@@ -165,9 +148,7 @@ int launch_stage(const wadg_ctx *c, int K, const double *vgeo, const double *vfg
     if (e != cudaSuccess) return cuda_check(e, "stage kernel smem attribute");
     attr.here() = true;
   }
-  const int per_sm = (int)((227 * 1024) / C::smem) > 0 ? (int)((227 * 1024) / C::smem) : 1;
-  const int batches = (K + C::E - 1) / C::E;
-  const int grid = batches < num_sms() * per_sm ? batches : num_sms() * per_sm;
+  const int grid = persistent_grid(K, C::E, C::smem);
   kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq,
                                                   Dsq, Dtq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, uq,
                                                   uf, Q, resQ, uq_out, uf_out, c->phys);
@@ -183,6 +164,63 @@ int launch_surf(const wadg_ctx *c, int K, const double *fgeo, const uint32_t *ma
   return after_launch("surf kernel");
 }
 
+// CTAs of the persistent update kernel: one per group of C::EW elements, at
+// most as many as are resident at once (occupancy, cached per device)
+template <int DIM, int N, bool CURVED>
+int update_grid(int K, int *grid) {
+  using C = UpdMmaCfg<DIM, N, CURVED>;
+  auto kern = update_mma_kernel<DIM, N, CURVED>;
+  static wadg_internal::PerDevice<int> per_sm_dev;
+  int &per_sm = per_sm_dev.here();
+  if (!per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    if (e != cudaSuccess) return cuda_check(e, "update kernel smem attribute");
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, C::threads, C::smem);
+    if (e != cudaSuccess) return cuda_check(e, "update kernel occupancy");
+    per_sm = n < 1 ? 1 : n;
+  }
+  const int ctas = (K + C::EW - 1) / C::EW;
+  *grid = ctas < num_sms() * per_sm ? ctas : num_sms() * per_sm;
+  return WADG_OK;
+}
+
+// the launch shape of one kernel for K elements (wadg_kernel_shape)
+template <int DIM, int N, bool CURVED, int W>
+void vol_shape(int K, int *E, int *grid) {
+  using C = VolPairsCfg<DIM, N, CURVED, W>;
+  *E = C::E;
+  *grid = persistent_grid(K, C::E, C::smem_vol);
+}
+
+template <int DIM, int N, bool CURVED>
+int kernel_shape(const wadg_ctx *c, int kernel, int K, int *E, int *grid) {
+  constexpr int W1 = volpairsW_cand<DIM, N, CURVED>(1), W2 = volpairsW_cand<DIM, N, CURVED>(2);
+  switch (kernel) {
+    case WADG_KERNEL_VOL:
+      if (W1 && c->vol_warps == W1) vol_shape<DIM, N, CURVED, (W1 ? W1 : 2)>(K, E, grid);
+      else if (W2 && c->vol_warps == W2) vol_shape<DIM, N, CURVED, (W2 ? W2 : 2)>(K, E, grid);
+      else vol_shape<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>(K, E, grid);
+      return WADG_OK;
+    case WADG_KERNEL_SURF:
+      *E = SurfMmaCfg<DIM, N>::EW;
+      *grid = (K + *E - 1) / *E;
+      return WADG_OK;
+    case WADG_KERNEL_UPDATE:
+      *E = UpdMmaCfg<DIM, N, CURVED>::EW;
+      return update_grid<DIM, N, CURVED>(K, grid);
+    case WADG_KERNEL_ADJ_PAIRS:
+      return wadg_internal::adj_pairs_shape(DIM, N, CURVED, K, E, grid);
+    case WADG_KERNEL_STAGE: {
+      using C = VolPairsCfg<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>;
+      *E = C::E;
+      *grid = persistent_grid(K, C::E, C::smem);
+      return WADG_OK;
+    }
+  }
+  return fail(WADG_ERR_INVALID, "unknown kernel %d", kernel);
+}
+
 template <int DIM, int N, bool CURVED>
 int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq,
                   const double *VfPq, double fa, double fb, double fdt, double *rhsQ,
@@ -190,43 +228,11 @@ int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq
   using C = UpdMmaCfg<DIM, N, CURVED>;
   static_assert(C::smem <= 227 * 1024, "update kernel does not fit in shared memory");
   auto kern = update_mma_kernel<DIM, N, CURVED>;
-  static wadg_internal::PerDevice<int> per_sm_dev;
-  int &per_sm = per_sm_dev.here();
-  if (!per_sm) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
-    if (e != cudaSuccess) return cuda_check(e, "update kernel smem attribute");
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, C::threads, C::smem);
-    if (e != cudaSuccess) return cuda_check(e, "update kernel occupancy");
-    if (per_sm < 1) per_sm = 1;
-  }
-  const int ctas = (K + C::EW - 1) / C::EW;
-  const int grid = ctas < num_sms() * per_sm ? ctas : num_sms() * per_sm;
+  int grid = 0;
+  if (int r = update_grid<DIM, N, CURVED>(K, &grid)) return r;
   kern<<<grid, C::threads, C::smem, c->stream>>>(K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q,
                                                  Qf, c->phys);
   return after_launch("update kernel");
-}
-
-// The volume kernel used by the entry points: vol_pairs (each volume-face
-// pair once) by default; WADG_VOL_KERNEL=rows selects the row-per-thread kernel.
-int vol_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("WADG_VOL_KERNEL");
-    v = (e && strcmp(e, "rows") == 0) ? 1 : 2;
-  }
-  return v;
-}
-
-template <int DIM, int N, bool CURVED>
-int vol_impl(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
-             const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
-             const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
-             const double *Qf, double *rhsQ, double *rhsQf) {
-  if (vol_variant() == 1)
-    return launch_vol<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
-                                      Qf, rhsQ, rhsQf);
-  return launch_vol_pairs<DIM, N, CURVED>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq,
-                                          VfPq, Qf, rhsQ, rhsQf);
 }
 
 // (dim, N) -> template instantiation
@@ -282,6 +288,9 @@ int wadg_ctx_sizes(const wadg_ctx *c, int *dim, int *NfqNf) {
   return WADG_OK;
 }
 
+// the stream a context's kernels run on (used by wadg_noalloc.cu)
+cudaStream_t wadg_ctx_stream(const wadg_ctx *c) { return c ? c->stream : nullptr; }
+
 // per-element integrals (wadg_euler_3d_compute_aux, wadg_element_entropy)
 template <int DIM, int N, bool ENTROPY>
 int launch_integral(const wadg_ctx *c, int K, const double *Jq, const double *wq, const double *Q,
@@ -304,6 +313,32 @@ __global__ void halo_pack_kernel(int n, int NF, int Nf, size_t nQf, const uint32
   const bool ok = sidx != 0xffffffffu && (size_t)sidx + (size_t)(Nf - 1) * NF < nQf;
   double *out = buf + (size_t)(g / NF) * NF * Nf + g % NF;
   for (int f = 0; f < Nf; ++f) out[(size_t)f * NF] = ok ? Qf[(size_t)sidx + (size_t)f * NF] : 0.0;
+}
+
+// failure detection: one thread per node of Q [K][Nf][Nq]; a node is bad when
+// a field is not finite, rho <= 0 or the pressure is <= 0.  work[0] counts the
+// bad nodes, work[1] keeps the smallest bad flat index k * Nq + i
+template <int DIM>
+__global__ void check_state_kernel(int K, int Nq, const double *__restrict__ Q, double gm1,
+                                   int *__restrict__ work) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)K * Nq) return;
+  const int k = (int)(t / Nq), i = (int)(t % Nq);
+  const double *q = Q + (size_t)k * Nq * (DIM + 2) + i;
+  const double rho = q[0], E = q[(size_t)(DIM + 1) * Nq];
+  bool finite = isfinite(rho) && isfinite(E);
+  double m2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double m = q[(size_t)(1 + d) * Nq];
+    finite = finite && isfinite(m);
+    m2 = fma(m, m, m2);
+  }
+  const double p = gm1 * (E - 0.5 * m2 / rho);
+  if (!finite || !(rho > 0.0) || !(p > 0.0)) {
+    atomicAdd(&work[0], 1);
+    atomicMin(&work[1], (int)t);
+  }
 }
 
 template <int DIM, int N, bool CURVED>
@@ -399,6 +434,17 @@ int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps) {
 
 int wadg_ctx_get_vol_warps(const wadg_ctx *ctx) { return ctx ? ctx->vol_warps : -1; }
 
+int wadg_kernel_shape(const wadg_ctx *ctx, int kernel, int curved, int K, int *elems_per_batch,
+                      int *grid) {
+  if (!ctx || !elems_per_batch || !grid) return fail(WADG_ERR_INVALID, "null argument");
+  if (K < 0) return fail(WADG_ERR_INVALID, "K < 0");
+  const wadg_ctx *c = ctx;
+  if (curved) {
+    WADG_DISPATCH(c, return (kernel_shape<D_, N_, true>(c, kernel, K, elems_per_batch, grid)));
+  }
+  WADG_DISPATCH(c, return (kernel_shape<D_, N_, false>(c, kernel, K, elems_per_batch, grid)));
+}
+
 // ------------------------------------------------------------------ diagnostics
 
 int wadg_euler_3d_compute_aux(wadg_ctx *c, int K, const double *Jq, const double *wq,
@@ -430,6 +476,36 @@ int wadg_halo_pack(wadg_ctx *c, int n, const uint32_t *src, const double *Qf, si
   return after_launch("halo pack kernel");
 }
 
+int wadg_check_state(wadg_ctx *c, int K, const double *Q, int *work, int *nbad, int *first) {
+  if (!c) return fail(WADG_ERR_INVALID, "null context");
+  if (K < 0) return fail(WADG_ERR_INVALID, "K < 0");
+  if (nbad) *nbad = 0;
+  if (first) *first = -1;
+  if (K == 0) return WADG_OK;
+  if (any_null({Q, work})) return fail(WADG_ERR_INVALID, "null pointer argument");
+  if ((long long)K * c->Nq >= 0x7f000000LL) return fail(WADG_ERR_INVALID, "K * Nq too large for a state check");
+  // work[1] starts at 0x7f7f7f7f, above every node index (byte-wise memset)
+  cudaError_t e = cudaMemsetAsync(work, 0, sizeof(int), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(work + 1, 0x7f, sizeof(int), c->stream);
+  if (e != cudaSuccess) return cuda_check(e, "state check memset");
+  const long long n = (long long)K * c->Nq;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (c->dim == 2)
+    check_state_kernel<2><<<blocks, 256, 0, c->stream>>>(K, c->Nq, Q, c->phys.gm1, work);
+  else
+    check_state_kernel<3><<<blocks, 256, 0, c->stream>>>(K, c->Nq, Q, c->phys.gm1, work);
+  if (int r = after_launch("state check kernel")) return r;
+  int h[2] = {0, 0};
+  e = cudaMemcpyAsync(h, work, sizeof h, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_check(e, "state check copy");
+  if (nbad) *nbad = h[0];
+  if (h[0] == 0) return WADG_OK;
+  if (first) *first = h[1];
+  return fail(WADG_ERR_STATE, "non-physical state: %d node(s) with a non-finite field, rho <= 0 or p <= 0; "
+              "first at element %d, node %d", h[0], h[1] / c->Nq, h[1] % c->Nq);
+}
+
 int wadg_entropy_rhs(wadg_ctx *c, int K, int curved, const double *wq, const double *Jq,
                      const double *VqPq, const double *Q, const double *rhs, double *out) {
   if (!c) return fail(WADG_ERR_INVALID, "null context");
@@ -454,7 +530,7 @@ int wadg_euler_vol_3d(wadg_ctx *c, int K, const double *vgeo, const double *vfge
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (vol_impl<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
+  WADG_DISPATCH(c, return (launch_vol_pairs<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
                                                     Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
@@ -468,7 +544,7 @@ int wadg_euler_vol_3d_curved(wadg_ctx *c, int K, const double *vgeo, const doubl
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (vol_impl<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
+  WADG_DISPATCH(c, return (launch_vol_pairs<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq,
                                                    Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
@@ -513,7 +589,7 @@ int wadg_euler_vol_2d(wadg_ctx *c, int K, const double *vgeo, const double *vfge
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (vol_impl<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
+  WADG_DISPATCH(c, return (launch_vol_pairs<D_, N_, false>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
                                                     Dsq, nullptr, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 
@@ -526,7 +602,7 @@ int wadg_euler_vol_2d_curved(wadg_ctx *c, int K, const double *vgeo, const doubl
   if (K == 0) return WADG_OK;
   if (any_null({vgeo, vfgeo, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ, rhsQf}))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  WADG_DISPATCH(c, return (vol_impl<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
+  WADG_DISPATCH(c, return (launch_vol_pairs<D_, N_, true>(c, K, vgeo, vfgeo, nrJ, nsJ, nullptr, Drq,
                                                    Dsq, nullptr, VqLq, VfPq, Qf, rhsQ, rhsQf)));
 }
 

@@ -57,8 +57,11 @@ int capture(wadg_ensemble *s, double dt) {
   e = cudaStreamEndCapture(s->master, &g);
   // capture issued but did not execute the stages: restore the bins' parity
   for (auto *a : s->bins) wadg_app_set_parity(a, p);
-  if (r) return r;
-  if (e != cudaSuccess) return efail(WADG_ERR_CUDA, "ensemble end capture", e);
+  if (e != cudaSuccess) return r ? r : efail(WADG_ERR_CUDA, "ensemble end capture", e);
+  if (r) {  // a stage failed to issue: drop the partial graph
+    cudaGraphDestroy(g);
+    return r;
+  }
   e = cudaGraphInstantiate(&s->graph[p], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return efail(WADG_ERR_CUDA, "ensemble instantiate", e);

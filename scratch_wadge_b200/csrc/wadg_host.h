@@ -45,4 +45,8 @@ inline int sm_count() {
   return c;
 }
 
+// launch shape (elements per batch, CTAs) of the adjoint's pair VJP kernel
+// for K elements (wadg_adjoint.cu)
+int adj_pairs_shape(int dim, int N, bool curved, int K, int *E, int *grid);
+
 }  // namespace wadg_internal

@@ -17,6 +17,7 @@
 // or several host threads) race on it: serialise them.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/wadg.h"
@@ -25,13 +26,14 @@ namespace wadg_internal {
 void set_error(const std::string &msg);  // wadg_capi.cu
 }
 int wadg_ctx_sizes(const wadg_ctx *c, int *dim, int *NfqNf);  // wadg_capi.cu
+cudaStream_t wadg_ctx_stream(const wadg_ctx *c);                // wadg_capi.cu
 
 namespace {
 
 __device__ __align__(256) double g_noalloc_scratch[WADG_NOALLOC_SCRATCH_DOUBLES];
 
 constexpr int kMaxDevices = 64;
-double *g_scratch_ptr[kMaxDevices] = {nullptr};
+std::atomic<double *> g_scratch_ptr[kMaxDevices];
 
 int nfail(int code, const std::string &msg) {
   wadg_internal::set_error(msg);
@@ -40,21 +42,30 @@ int nfail(int code, const std::string &msg) {
 
 // The device address of the scratch array on the current device.  In host
 // code `g_noalloc_scratch` names a host-side stand-in, not device memory, so
-// the address is looked up once per device (with that device current) and
-// cached.
-int scratch_on_current_device(double **out) {
+// the address is looked up with that device current.  The lookup is repeated
+// on every call whose stream is not being captured (a context torn down and
+// made again, e.g. by cudaDeviceReset, reloads the module at a new address);
+// during a capture the address found by the last call on this device is
+// used, so the first call on a device has to come before any capture.
+int scratch_on_current_device(cudaStream_t stream, double **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return nfail(WADG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return nfail(WADG_ERR_UNSUPPORTED, "device ordinal out of range");
-  if (!g_scratch_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cs);
+  if (e != cudaSuccess)
+    return nfail(WADG_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+  double *p = g_scratch_ptr[dev].load(std::memory_order_acquire);
+  if (cs == cudaStreamCaptureStatusNone || !p) {
+    void *a = nullptr;
+    e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
     if (e != cudaSuccess)
       return nfail(WADG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch_ptr[dev] = static_cast<double *>(p);
+    p = static_cast<double *>(a);
+    g_scratch_ptr[dev].store(p, std::memory_order_release);
   }
-  *out = g_scratch_ptr[dev];
+  *out = p;
   return WADG_OK;
 }
 
@@ -81,7 +92,7 @@ extern "C" int wadg_rk_stage_noalloc(wadg_ctx *ctx, int K, int curved, const dou
                      std::to_string((size_t)WADG_NOALLOC_SCRATCH_DOUBLES) +
                      " (use wadg_app or the kernel entry points with your own rhsQf)");
   double *rhsQf = nullptr;
-  if (int r = scratch_on_current_device(&rhsQf)) return r;
+  if (int r = scratch_on_current_device(wadg_ctx_stream(ctx), &rhsQf)) return r;
 
   int r;
   if (dim == 3) {

@@ -1,8 +1,8 @@
 // Pair-scheduled volume kernel (the default volume kernel) and the fused
 // stage kernel built on it.
 //
-// Same mathematics as vol_kernel (wadg_kernels.cuh), organised so that every
-// volume-face pair (i, f) is evaluated once: F_S(u_i, uf_f).nJ_f feeds both
+// The reference's volume kernels (one thread per row, Euler3Daffine.okl:152-417),
+// organised so that every volume-face pair (i, f) is evaluated once: F_S(u_i, uf_f).nJ_f feeds both
 // the volume row i (weight 1/2 VqLq_if) and the face row f (weight
 // -1/2 VfPq_fi).  The reference evaluates it twice, once per row
 // (Euler3Daffine.okl:327-362 and :387-406); the flux is symmetric in its two
@@ -367,6 +367,10 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
 
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
     if (PRE) cp_async_wait_all();
+    // a group whose elements all lie past the end (the CTA's last batch) has
+    // nothing to compute, and must not read element K-1's input, which the
+    // group owning it may already have overwritten with its RHS
+    if (k0 + q * G >= K) break;
     gsync();  // the group's traces staged / its previous batch done with its shared memory
     v.prologue_range(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P, PRE ? v.sPre : nullptr);
     gsync();
@@ -440,6 +444,7 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
   __syncthreads();  // the tables are shared by every group
 
   for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
+    if (k0 + e0 >= K) break;  // the group's elements all lie past the end
     gsync();
     v.prologue_range(K, k0, e0, G, tid, nth, vgeo, vfgeo, uq, uf, P, nullptr);
     gsync();

@@ -75,6 +75,8 @@ def concat(parts):
     offs = np.cumsum([0] + [g.K for g in geos])
     per = ops.NfqNf * ops.Nfields
     mapPq = np.concatenate([g.mapPq.astype(np.int64) + o * per for g, o in zip(geos, offs[:-1])])
+    if int(offs[-1]) * per > 2 ** 32:
+        raise ValueError(f"bin of {int(offs[-1])} elements: neighbour indices exceed the 32-bit mapPq")
     cat = lambda name: np.concatenate([getattr(g, name) for g in geos])
     geo = M.Geometry(ops, int(offs[-1]), cat("vgeo"), cat("vfgeo"), cat("fgeo"), cat("Jq"),
                      mapPq.astype(np.uint32), cat("xyzq"), cat("xyzf"))

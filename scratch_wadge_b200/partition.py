@@ -249,7 +249,10 @@ def run_local(parts: list, dt: float, nsteps: int) -> None:
 def run_dist(part: Part, dt: float, nsteps: int, group=None) -> None:
     """nsteps LSRK-45 time steps of this rank's part.  The halo exchange of a
     stage runs while its volume kernel does (only the surface kernel reads
-    the ghosts)."""
+    the ghosts).  The part's kernels run on torch's current stream, the
+    stream the collective is ordered on."""
+    import torch
+    part.ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     for _ in range(nsteps):
         for st in range(5):
             work = exchange_dist(part, group, async_op=True)

@@ -90,3 +90,24 @@ def test_diagnostic_and_halo_validation(L):
     assert L.wadg_halo_pack(h, -48, 8, 8, 100, 8) == 1
     assert L.wadg_halo_pack(h, 48, None, 8, 100, 8) == 1
     L.wadg_ctx_destroy(h)
+
+
+def test_state_check_and_shape_validation(L):
+    """wadg_check_state and wadg_kernel_shape reject bad arguments before any
+    CUDA call; an empty state is physical."""
+    ops = R.load(3, 3)
+    h = ctypes.c_void_p()
+    p = capi.params_for(ops)
+    assert L.wadg_ctx_create(ctypes.byref(p), ctypes.byref(h)) == 0
+    nbad, first = ctypes.c_int(7), ctypes.c_int(7)
+    assert L.wadg_check_state(h, 0, None, None, ctypes.byref(nbad), ctypes.byref(first)) == 0
+    assert nbad.value == 0 and first.value == -1
+    assert L.wadg_check_state(h, -1, None, None, None, None) == capi.ERR_INVALID
+    assert L.wadg_check_state(h, 4, None, 8, None, None) == capi.ERR_INVALID
+    assert L.wadg_check_state(None, 4, 8, 8, None, None) == capi.ERR_INVALID
+    E, g = ctypes.c_int(), ctypes.c_int()
+    assert L.wadg_kernel_shape(h, 9, 0, 10, ctypes.byref(E), ctypes.byref(g)) == capi.ERR_INVALID
+    assert b"unknown kernel" in L.wadg_last_error()
+    assert L.wadg_kernel_shape(h, 0, 0, -1, ctypes.byref(E), ctypes.byref(g)) == capi.ERR_INVALID
+    assert L.wadg_kernel_shape(h, 0, 0, 10, None, ctypes.byref(g)) == capi.ERR_INVALID
+    L.wadg_ctx_destroy(h)

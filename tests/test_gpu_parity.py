@@ -233,9 +233,11 @@ def test_entropy_dissipation_2d(cuda):
     assert S > 0
 
 
-@pytest.mark.parametrize("name", ["tg3d_affine_N3", "tg3d_affine_N2", "vortex2d_affine_N2"])
+@pytest.mark.parametrize("name", ["tg3d_affine_N3", "tg3d_affine_N2", "vortex2d_affine_N2",
+                                  "dw3d_curved_N3", "dw3d_curved_N4", "vortex2d_curved_N3"])
 def test_device_projection_matches_stage0(cuda, name):
-    """wadg_app_project = the reference's stage-0 builder (affine meshes)."""
+    """wadg_app_project = the reference's stage-0 builder, which projects with
+    VqPq alone on curved meshes too (euler.c:3958-4133)."""
     c = Case(name)
     app = capi.App(c.geo, c.curved)
     st = c.state()
@@ -246,7 +248,8 @@ def test_device_projection_matches_stage0(cuda, name):
     assert np.array_equal(out["Q"], st["Q"]) and not out["resQ"].any()
 
 
-@pytest.mark.parametrize("name", ["tg3d_affine_N3", "vortex2d_affine_N2"])
+@pytest.mark.parametrize("name", ["tg3d_affine_N3", "vortex2d_affine_N2", "dw3d_curved_N4",
+                                  "vortex2d_curved_N3"])
 def test_solve_from_q_equals_solve_from_stage0_state(cuda, name):
     c = Case(name)
     app = capi.App(c.geo, c.curved)

@@ -69,3 +69,107 @@ def test_partitioned_run_equals_single_domain(cuda, name, nparts):
     for p in parts:
         p.close()
     assert np.array_equal(got, ref), float(np.abs(got - ref).max() / np.abs(ref).max())
+
+
+class _FakeAllToAll:
+    """dist.all_to_all_single for ranks that are threads of one process, each
+    on its own CUDA stream: a rank's call records an event on its current
+    stream (after its pack), all ranks meet on the host, then one side stream
+    waits for every rank's event and copies every block into its receiver's
+    ghost region; the returned work's wait() makes the caller's current
+    stream wait for those copies (so a rank's send buffer is free again and
+    its ghosts are filled, as when an NCCL all-to-all completes)."""
+
+    def __init__(self, torch, nranks):
+        import threading
+        self.torch, self.n = torch, nranks
+        self.bar = threading.Barrier(nranks)
+        self.side = torch.cuda.Stream()
+        self.slots = [None] * nranks
+        self.done = None
+
+    def __call__(self, rank):
+        torch = self.torch
+
+        def a2a(output, input, output_split_sizes, input_split_sizes, group=None, async_op=False):
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream())
+            self.slots[rank] = (output, input, list(output_split_sizes), list(input_split_sizes), ev)
+            self.bar.wait()
+            if rank == 0:
+                with torch.cuda.stream(self.side):
+                    for *_, e in self.slots:
+                        self.side.wait_event(e)
+                    for r, (out, _, osz, _, _) in enumerate(self.slots):
+                        ro = np.concatenate([[0], np.cumsum(osz)])
+                        for s_, (_, inp, _, isz, _) in enumerate(self.slots):
+                            io = np.concatenate([[0], np.cumsum(isz)])
+                            n = int(io[r + 1] - io[r])
+                            assert n == int(ro[s_ + 1] - ro[s_])
+                            if n:
+                                out[int(ro[s_]):int(ro[s_ + 1])].copy_(inp[int(io[r]):int(io[r + 1])])
+                    self.done = torch.cuda.Event()
+                    self.done.record(self.side)
+            self.bar.wait()
+            done = self.done
+
+            class Work:
+                def wait(self_):
+                    torch.cuda.current_stream().wait_event(done)
+
+            self.bar.wait()  # every rank holds this exchange's event before the next one
+            return Work()
+
+        return a2a
+
+
+def test_run_dist_stream_ordering_with_a_fake_collective(cuda, monkeypatch):
+    """run_dist (the overlapped exchange of partitioned multi-GPU runs) with
+    two ranks as threads, each on its own stream, and the collective replaced
+    by device copies on a third stream: the result equals the single-domain
+    run bit for bit, so pack -> exchange -> surface are ordered right."""
+    import threading
+
+    import torch.distributed as dist
+    mesh, N, curved, kind, kw = _case("tg3d_N3")
+    geo = M.build_geometry(mesh, N)
+    Q, rhsQ, Qf, resQ = IC.stage0(geo, IC.initial_state(geo, kind, **kw))
+    dt = IC.time_step(geo, 0.5, N, nsteps=1, wave_speed=IC.max_wave_speed(Q))[0]
+    app = capi.App(geo, curved)
+    app.set_state(Q, rhsQ, Qf, resQ)
+    app.rk_run(dt, 3, graph=False)
+    ref = app.get_state()["Q"]
+    app.close()
+    state = dict(Q=Q, rhsQ=rhsQ, Qf=Qf, resQ=resQ)
+    fake = _FakeAllToAll(cuda, 2)
+    streams = [cuda.cuda.Stream() for _ in range(2)]
+    parts = []
+    for r, p in enumerate(PT.plan(geo, 2)):
+        with cuda.cuda.stream(streams[r]):
+            parts.append(PT.Part(geo, p, state, curved))
+    cuda.cuda.synchronize()
+    local = threading.local()
+    monkeypatch.setattr(dist, "all_to_all_single",
+                        lambda *a, **k: fake(local.rank)(*a, **k))
+    errors = []
+
+    def rank_main(r):
+        local.rank = r
+        try:
+            with cuda.cuda.stream(streams[r]):
+                PT.run_dist(parts[r], dt, 3)
+        except Exception as e:  # surfaced by the main thread
+            errors.append(e)
+            fake.bar.abort()
+
+    th = [threading.Thread(target=rank_main, args=(r,)) for r in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(120)
+    assert not errors, errors
+    cuda.cuda.synchronize()
+    got = PT.gather_Q(parts, geo.K)
+    for p in parts:
+        p.close()
+    assert np.array_equal(got, ref), float(np.abs(got - ref).max() / np.abs(ref).max())

@@ -55,3 +55,17 @@ def test_single_process_needs_no_group(monkeypatch):
     assert pg is None
     assert RP.all_max(pg, 3.5) == 3.5 and RP.agree(pg, True) is True
     RP.finish(pg)
+
+
+def test_bench_refuses_a_rank_count_other_than_gpus():
+    """bench.py --gpus N under a launcher that started a different number of
+    ranks exits non-zero before any GPU work (it would otherwise report one
+    GPU's throughput as N GPUs')."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, WORLD_SIZE="3", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2"], env=env,
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0 and "WORLD_SIZE=3" in r.stderr
