@@ -99,6 +99,9 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     d = Dev(cuda, geo, curved)
     ref = oracle(ops, curved)
     st = state(geo, curved, 5)
+    # a stable step for the mesh (the finer the mesh, the smaller), so that
+    # the update of these rough states stays physical
+    dt = IC.time_step(geo, 0.1, N, nsteps=1, wave_speed=IC.max_wave_speed(st["Q"]))[0]
 
     # volume kernel, every compiled CTA shape
     for w, E, g in sh:
@@ -127,7 +130,7 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     d.ctx.surf(K, d.g["fgeo"].data_ptr(), d.g["mapPq"].data_ptr(), d.g["VqLq"].data_ptr(),
                s["Qf"].data_ptr(), s["rhsQf"].data_ptr(), s["rhsQ"].data_ptr())
     d.ctx.update(curved, K, d.g["Jq"].data_ptr(), d.g["VqPq"].data_ptr(), d.g["VfPq"].data_ptr(),
-                 IC.RK4A[2], IC.RK4B[2], 1e-3, s["rhsQ"].data_ptr(), s["resQ"].data_ptr(),
+                 IC.RK4A[2], IC.RK4B[2], dt, s["rhsQ"].data_ptr(), s["resQ"].data_ptr(),
                  s["Q"].data_ptr(), s["Qf"].data_ptr())
     d.sync()
     h = d.get(s)
@@ -136,8 +139,9 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     # whole trace array, updating only the first K elements
     Qf_all = np.ascontiguousarray(st["Qf"]).copy()
     ref.surf(geo, Qf_all, a["rhsQf"], a["rhsQ"])
-    ref.update(geo, IC.RK4A[2], IC.RK4B[2], 1e-3, a["rhsQ"], a["resQ"], a["Q"], a["Qf"])
+    ref.update(geo, IC.RK4A[2], IC.RK4B[2], dt, a["rhsQ"], a["resQ"], a["Q"], a["Qf"])
     for k in ("Q", "rhsQ", "Qf", "resQ"):
+        assert np.isfinite(a[k]).all(), k
         assert rel(h[k][:K], a[k]) < RTOL, (k, rel(h[k][:K], a[k]))
         assert np.array_equal(h[k][K:], st[k][K:]), k
 
@@ -151,7 +155,7 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     args += [g["ntJ"].data_ptr()] if dim == 3 else []
     args += [g["Drq"].data_ptr(), g["Dsq"].data_ptr()] + ([g["Dtq"].data_ptr()] if dim == 3 else [])
     args += [g[n].data_ptr() for n in ("VqLq", "VfPq", "VqPq", "Jq")]
-    capi.check(fn(d.ctx.h, K, int(curved), *args, IC.RK4A[3], IC.RK4B[3], 1e-3, s["rhsQ"].data_ptr(),
+    capi.check(fn(d.ctx.h, K, int(curved), *args, IC.RK4A[3], IC.RK4B[3], dt, s["rhsQ"].data_ptr(),
                   s["Qf"].data_ptr(), s["Q"].data_ptr(), s["resQ"].data_ptr(), out["rhsQ"].data_ptr(),
                   out["Qf"].data_ptr()), "stage")
     d.sync()
@@ -160,10 +164,11 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     Qf_all = np.ascontiguousarray(st["Qf"]).copy()
     ref.vol(geo, a["Qf"], a["rhsQ"], a["rhsQf"])
     ref.surf(geo, Qf_all, a["rhsQf"], a["rhsQ"])
-    ref.update(geo, IC.RK4A[3], IC.RK4B[3], 1e-3, a["rhsQ"], a["resQ"], a["Q"], a["Qf"])
+    ref.update(geo, IC.RK4A[3], IC.RK4B[3], dt, a["rhsQ"], a["resQ"], a["Q"], a["Qf"])
     got = dict(Q=s["Q"].cpu().numpy(), resQ=s["resQ"].cpu().numpy(), rhsQ=out["rhsQ"].cpu().numpy(),
                Qf=out["Qf"].cpu().numpy())
     for k in ("Q", "rhsQ", "Qf", "resQ"):
+        assert np.isfinite(a[k]).all(), k
         assert rel(got[k][:K], a[k]) < RTOL, (k, rel(got[k][:K], a[k]))
     assert np.array_equal(got["Q"][K:], st["Q"][K:])
     assert (got["rhsQ"][K:] == SENTINEL).all() and (got["Qf"][K:] == SENTINEL).all()
