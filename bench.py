@@ -59,6 +59,9 @@ METRIC = "FP64 DOF*stages/s at N=3 (3D affine-tet Taylor-Green, Euler3Daffine RH
 UNIT = "DOF*stages/s"
 WORKLOAD = "taylor_green_3d_affine_N3_K24576"
 NHEX, N, CFL, E2E_STEPS = 16, 3, 0.5, 100
+# stage implementations the time step can run, and kernel launches per step
+VARIANTS = ["three_kernels", "fused", "volsurf"]
+LAUNCHES = {"three_kernels": 15, "fused": 5, "volsurf": 10}
 
 
 def dist_env():
@@ -255,18 +258,20 @@ def run_ours(args):
     vol_warps, vol_cand = app.autotune(dt)
     app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     # warm-up (also captures the time-step graphs) and the choice between the
-    # two stage implementations: three reference kernels or the fused kernel
+    # stage implementations: three reference kernels, the fused kernel, or
+    # the volume + surface kernel and the update kernel
     variants = {}
-    for fused in (False, True):
-        app.set_fused(fused)
+    for name in VARIANTS:
+        app.set_stage_variant(name)
         app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
         app.rk_run(dt, max(args.warmup, 1), graph=True)
-        variants["fused" if fused else "three_kernels"] = app.time_run(dt, 10, graph=True) / 10
-    use_fused = variants["fused"] < variants["three_kernels"]
+        variants[name] = app.time_run(dt, 10, graph=True) / 10
+    pick = min(VARIANTS, key=lambda n: variants[n])
     if args.stage_variant != "auto":  # pinned (profiling: timings under a profiler mislead the choice)
-        use_fused = args.stage_variant == "fused"
-    use_fused = RP.agree(pg, use_fused)  # every rank takes the same variant
-    app.set_fused(use_fused)
+        pick = args.stage_variant
+    # every rank takes the same variant (rank 0's choice)
+    pick = VARIANTS[int(RP.all_max(pg, VARIANTS.index(pick) if rank == 0 else 0))]
+    app.set_stage_variant(pick)
     app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     app.rk_run(dt, max(args.warmup, 1), graph=True)
     barrier()
@@ -289,30 +294,44 @@ def run_ours(args):
     stage_ms = app.time_stage(dt, nst) / nst
     kms = app.time_kernels(dt, nst)
     vol_ms, surf_ms, upd_ms = (x / nst for x in kms)
+    vs_ms, vs_upd_ms = (x / nst for x in app.time_volsurf(dt, nst))
     fl_stage = RF.stage_flops_per_element(3, Nq, NfqNf, False) * K
+    fl_vs = RF.volsurf_flops_per_element(3, Nq, NfqNf, False) * K
     fl = RF.vol_flops_per_element(3, Nq, NfqNf, False) * K
     probe = fp64_peak(stream)
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
+    prof = ncu_traffic()
     # the roofline line describes the dominant kernel of the variant the time
-    # step ran: the fused stage kernel, or the volume kernel of the three
-    if use_fused:
-        achieved = fl_stage / (stage_ms * 1e-3) / 1e12
+    # step ran: the fused stage kernel, the volume + surface kernel, or the
+    # volume kernel of the three
+    if pick == "fused":
         roof = {"kernel": "stage_kernel (fused vol + surf + update, one launch per LSRK stage)",
                 "algorithmic_flops_per_launch": fl_stage, "launch_ms": stage_ms,
                 "flops_per_element": RF.stage_flops_per_element(3, Nq, NfqNf, False),
-                "traffic": ncu_traffic().get("stage_3d_affine_N3_K24576")}
+                "ncu": prof.get("stage_3d_affine_N3_K24576")}
+    elif pick == "volsurf":
+        roof = {"kernel": "vol_pairs_kernel<SURF> (wadg_euler_volsurf_3d: volume pairs, surface "
+                          "flux and lift in one launch)",
+                "algorithmic_flops_per_launch": fl_vs, "launch_ms": vs_ms,
+                "flops_per_element": RF.volsurf_flops_per_element(3, Nq, NfqNf, False),
+                "ncu": prof.get("volsurf_3d_affine_N3_K24576")}
     else:
-        achieved = fl / (vol_ms * 1e-3) / 1e12
         roof = {"kernel": "vol_pairs_kernel (euler_vol_3d, the pair-scheduled volume kernel)",
                 "algorithmic_flops_per_launch": fl, "launch_ms": vol_ms,
                 "flops_per_element": RF.vol_flops_per_element(3, Nq, NfqNf, False),
-                "traffic": ncu_traffic().get("vol_3d_affine_N3_K24576")}
+                "ncu": prof.get("vol_3d_affine_N3_K24576")}
+    achieved = roof["algorithmic_flops_per_launch"] / (roof["launch_ms"] * 1e-3) / 1e12
+    ncu = roof.pop("ncu") or {}
     roof.update({"bound": "fp64", "achieved": achieved, "peak": probe, "unit": "TFLOP/s",
                  "frac": achieved / probe,
                  "peak_source": "measured in-run: FP64 FMA probe (wadg_probe_fp64_fma)",
+                 "traffic": ncu.get("dram_bytes"),
+                 "ncu_fp64_pipe_active": ncu.get("fp64_pipe_active"),
+                 "ncu_source": ncu.get("source"),
                  "pairs_per_element": RF.pairs_per_element(Nq, NfqNf),
-                 "other_variant_stage_ms": vol_ms + surf_ms + upd_ms if use_fused else stage_ms})
+                 "stage_ms": {"three_kernels": vol_ms + surf_ms + upd_ms, "fused": stage_ms,
+                              "volsurf": vs_ms + vs_upd_ms}})
     sb = RF.surf_bytes_per_element(3, Nq, NfqNf) * K
     ub = RF.update_bytes_per_element(3, Nq, NfqNf) * K
     hbm_kernels = {
@@ -354,11 +373,10 @@ def run_ours(args):
                             f"on the device, {E2E_STEPS} time steps, D2H of Q (pinned host "
                             f"buffers, wall clock)",
                     "calls": e2e_calls},
-            "gpu_launches": (5 if use_fused else 15) * args.steps,
+            "gpu_launches": LAUNCHES[pick] * args.steps,
             "autotune": {"vol_warps": vol_warps,
                          "vol_ms_per_candidate": {str(w): t for w, t in vol_cand.items()}},
-            "stage_variant": {"used": "fused" if use_fused else "three_kernels",
-                              "ms_per_step": variants},
+            "stage_variant": {"used": pick, "ms_per_step": variants},
             "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks, "setup": setup}
     if not args.no_ensemble:
         line["ensemble"] = run_ensemble_measurement()
@@ -535,7 +553,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--stage-variant", choices=["auto", "three_kernels", "fused"], default="auto",
+    ap.add_argument("--stage-variant", choices=["auto"] + VARIANTS, default="auto",
                     help="stage implementation of the time step (auto: the faster one, timed)")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + steps of the device path (for ncu), no JSON line")

@@ -82,7 +82,8 @@ enum
   WADG_KERNEL_SURF = 1,
   WADG_KERNEL_UPDATE = 2,
   WADG_KERNEL_STAGE = 3,
-  WADG_KERNEL_ADJ_PAIRS = 4 /* the adjoint's pair VJP kernel (persistent) */
+  WADG_KERNEL_ADJ_PAIRS = 4, /* the adjoint's pair VJP kernel (persistent) */
+  WADG_KERNEL_VOLSURF = 5    /* the volume + surface kernel (persistent) */
 };
 int wadg_kernel_shape(const wadg_ctx *ctx, int kernel, int curved, int K, int *elems_per_batch,
                       int *grid);
@@ -319,6 +320,30 @@ int wadg_euler_stage_2d(wadg_ctx *ctx, int K, int curved, const double *vgeo,
                         const double *Qf_in, double *Q, double *resQ,
                         double *rhsQ_out, double *Qf_out);
 
+/* ------------------------------------------------------------ volume + surface
+ * The first two launches of rk_step (euler_vol_* then euler_surf_*,
+ * euler.c:3615-3640) in one: rhsQ holds u~ on entry and, on exit, the whole
+ * right-hand side the surface kernel leaves (volume rows plus the lift of the
+ * surface flux, penalty and face rows); the face rows stay on chip, so no
+ * rhsQf buffer.  Qf (the traces of every element, read for the neighbour
+ * gathers) is only read.  Arguments are those of the two kernels; the update
+ * kernel follows as before.  Sums run in another order than the two kernels',
+ * so results agree with them to rounding.  No single-kernel counterpart in
+ * the reference. */
+int wadg_euler_volsurf_3d(wadg_ctx *ctx, int K, int curved, const double *vgeo,
+                          const double *vfgeo, const double *fgeo,
+                          const uint32_t *mapPq, const double *nrJ,
+                          const double *nsJ, const double *ntJ,
+                          const double *Drq, const double *Dsq,
+                          const double *Dtq, const double *VqLq,
+                          const double *VfPq, const double *Qf, double *rhsQ);
+int wadg_euler_volsurf_2d(wadg_ctx *ctx, int K, int curved, const double *vgeo,
+                          const double *vfgeo, const double *fgeo,
+                          const uint32_t *mapPq, const double *nrJ,
+                          const double *nsJ, const double *Drq,
+                          const double *Dsq, const double *VqLq,
+                          const double *VfPq, const double *Qf, double *rhsQ);
+
 /* ------------------------------------------------------------ host driver
  * The reference's app_t / rk_step / rk_run (euler.c:2607-2796, 3610-3738)
  * over device buffers owned by the library.  Host arrays are copied once at
@@ -379,10 +404,18 @@ int wadg_app_project(wadg_app *app);
 int wadg_app_solve_host_q(wadg_app *app, const double *Q0, double dt,
                           int nsteps, double *Q);
 int wadg_app_sync(wadg_app *app);
-/* fused != 0: wadg_rk_step / wadg_rk_run launch the fused stage kernel (one
- * launch per stage, ping-pong state buffers); 0 (the default): the three
- * reference kernels per stage.  Results agree to rounding. */
-int wadg_app_set_fused(wadg_app *app, int fused);
+/* The stage variant wadg_rk_step / wadg_rk_run launch:
+ * WADG_STAGE_THREE (0, the default): the three reference kernels;
+ * WADG_STAGE_FUSED (1): the fused stage kernel (one launch per stage,
+ * ping-pong state buffers); WADG_STAGE_VOLSURF (2): the volume + surface
+ * kernel, then the update kernel.  Results agree to rounding. */
+enum
+{
+  WADG_STAGE_THREE = 0,
+  WADG_STAGE_FUSED = 1,
+  WADG_STAGE_VOLSURF = 2
+};
+int wadg_app_set_fused(wadg_app *app, int variant);
 /* device pointers of the state arrays (for zero-copy use and testing) */
 int wadg_app_state_ptrs(wadg_app *app, double **Q, double **rhsQ, double **Qf,
                         double **resQ, double **rhsQf);
@@ -396,6 +429,9 @@ int wadg_app_time_kernels(wadg_app *app, double dt, int nstages, float *ms);
 /* Time `nstages` fused stage launches (CUDA events around the sequence);
  * ms receives the total. */
 int wadg_app_time_stage(wadg_app *app, double dt, int nstages, float *ms);
+/* Time `nstages` stages of the volume + surface variant with CUDA events
+ * around every launch; ms[0..1] = total volume + surface, update time. */
+int wadg_app_time_volsurf(wadg_app *app, double dt, int nstages, float *ms);
 
 /* Autotuner: times `nstages` LSRK stages (three kernels, CUDA events) with
  * each compiled CTA shape of the volume kernel on the app's own mesh and

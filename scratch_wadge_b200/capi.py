@@ -85,6 +85,9 @@ def lib():
         L.wadg_euler_stage_2d.argtypes = [v, i, i] + [v] * 12 + [d, d, d] + [v] * 6
         L.wadg_app_set_fused.argtypes = [v, i]
         L.wadg_app_time_stage.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
+        L.wadg_app_time_volsurf.argtypes = [v, d, i, ctypes.POINTER(ctypes.c_float)]
+        L.wadg_euler_volsurf_3d.argtypes = [v, i, i] + [v] * 14
+        L.wadg_euler_volsurf_2d.argtypes = [v, i, i] + [v] * 12
         L.wadg_probe_fp64_fma.argtypes = [v, i, ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_float)]
         L.wadg_app_ctx.restype = ctypes.c_void_p
@@ -197,6 +200,17 @@ class Context:
                                         Drq, Dsq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, rhsQ_in, Qf_in,
                                         Q, resQ, rhsQ_out, Qf_out), "stage")
 
+    def volsurf(self, curved, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq,
+                Qf, rhsQ):
+        """The volume + surface kernel (wadg_euler_volsurf_3d/_2d)."""
+        L = lib()
+        if self.ops.dim == 3:
+            check(L.wadg_euler_volsurf_3d(self.h, K, int(curved), vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ,
+                                          Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ), "volsurf")
+        else:
+            check(L.wadg_euler_volsurf_2d(self.h, K, int(curved), vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                          Drq, Dsq, VqLq, VfPq, Qf, rhsQ), "volsurf")
+
     def compute_aux(self, K, Jq, wq, Q, aux):
         """per-element kinetic energy (euler_3d_compute_aux)"""
         check(lib().wadg_euler_3d_compute_aux(self.h, K, Jq, wq, Q, aux), "compute_aux")
@@ -223,7 +237,7 @@ class Context:
             check(r, "check_state")
         return r, nbad.value, first.value
 
-    KERNELS = {"vol": 0, "surf": 1, "update": 2, "stage": 3, "adj_pairs": 4}
+    KERNELS = {"vol": 0, "surf": 1, "update": 2, "stage": 3, "adj_pairs": 4, "volsurf": 5}
 
     def shape(self, kernel, curved, K):
         """(elements per batch, CTAs launched) of `kernel` for K elements
@@ -357,10 +371,24 @@ class App:
         check(lib().wadg_app_time_run(self.h, dt, nsteps, int(graph), ctypes.byref(ms)), "time_run")
         return ms.value
 
+    STAGE_VARIANTS = {"three_kernels": 0, "fused": 1, "volsurf": 2}
+
     def set_fused(self, fused: bool):
         """fused stage kernel (one launch per stage) or, the default, the three
         reference kernels per stage"""
-        check(lib().wadg_app_set_fused(self.h, int(fused)), "set_fused")
+        check(lib().wadg_app_set_fused(self.h, int(bool(fused))), "set_fused")
+
+    def set_stage_variant(self, name: str):
+        """the stage the time loop launches: "three_kernels" (vol, surf,
+        update), "fused" (one launch) or "volsurf" (volume + surface, then
+        update)"""
+        check(lib().wadg_app_set_fused(self.h, self.STAGE_VARIANTS[name]), "set_stage_variant")
+
+    def time_volsurf(self, dt, nstages):
+        """(volume + surface ms, update ms) summed over nstages stages"""
+        ms = (ctypes.c_float * 2)()
+        check(lib().wadg_app_time_volsurf(self.h, dt, nstages, ms), "time_volsurf")
+        return ms[0], ms[1]
 
     def time_stage(self, dt, nstages):
         ms = ctypes.c_float()

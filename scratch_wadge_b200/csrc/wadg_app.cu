@@ -125,8 +125,27 @@ int stage_fused(wadg_app *a, double rka, double rkb, double dt) {
   return r;
 }
 
+// the volume + surface kernel on the current buffers (rhsQ: u~ in, RHS out)
+int volsurf(wadg_app *a) {
+  double *rhsQ = a->uq[a->cur], *Qf = a->uf[a->cur];
+  return a->p.dim == 3
+             ? wadg_euler_volsurf_3d(a->ctx, a->K, a->curved, a->vgeo, a->vfgeo, a->fgeo, a->mapPq,
+                                     a->nrJ, a->nsJ, a->ntJ, a->Drq, a->Dsq, a->Dtq, a->VqLq,
+                                     a->VfPq, Qf, rhsQ)
+             : wadg_euler_volsurf_2d(a->ctx, a->K, a->curved, a->vgeo, a->vfgeo, a->fgeo, a->mapPq,
+                                     a->nrJ, a->nsJ, a->Drq, a->Dsq, a->VqLq, a->VfPq, Qf, rhsQ);
+}
+
+int stage_volsurf(wadg_app *a, double rka, double rkb, double dt) {
+  int r = volsurf(a);
+  if (!r) r = update(a, rka, rkb, dt, a->curved);
+  return r;
+}
+
 int stage(wadg_app *a, double rka, double rkb, double dt) {
-  return a->fused ? stage_fused(a, rka, rkb, dt) : stage3(a, rka, rkb, dt);
+  if (a->fused == WADG_STAGE_FUSED) return stage_fused(a, rka, rkb, dt);
+  if (a->fused == WADG_STAGE_VOLSURF) return stage_volsurf(a, rka, rkb, dt);
+  return stage3(a, rka, rkb, dt);
 }
 
 // capture one time step (5 stages) starting from buffer parity a->cur; the
@@ -323,7 +342,7 @@ int wadg_rk_run(wadg_app *a, double dt, int nsteps, int use_graph) {
       if (r) return r;
       cudaError_t e = cudaGraphLaunch(a->graph[p], a->stream);
       if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "cudaGraphLaunch", e);
-      if (a->fused) a->cur = 1 - p;  // 5 stages flip the parity once
+      if (a->fused == WADG_STAGE_FUSED) a->cur = 1 - p;  // 5 stages flip the parity once
     } else {
       for (int s = 0; s < 5; ++s)
         if (int r = stage(a, RK4A[s], RK4B[s], dt)) return r;
@@ -345,9 +364,11 @@ int wadg_app_check_state(wadg_app *a, int *nbad, int *first) {
   return wadg_check_state(a->ctx, a->K, a->Q, a->check_work, nbad, first);
 }
 
-int wadg_app_set_fused(wadg_app *a, int fused) {
+int wadg_app_set_fused(wadg_app *a, int variant) {
   if (!a) return afail(WADG_ERR_INVALID, "null app");
-  a->fused = fused ? 1 : 0;
+  if (variant < WADG_STAGE_THREE || variant > WADG_STAGE_VOLSURF)
+    return afail(WADG_ERR_INVALID, "unknown stage variant");
+  a->fused = variant;
   return WADG_OK;
 }
 
@@ -413,7 +434,7 @@ int wadg_app_time_run(wadg_app *a, double dt, int nsteps, int use_graph, float *
   if (use_graph) {  // instantiate both parities' graphs outside the timed region
     int r = capture_step(a, dt);
     if (r) return r;
-    if (a->fused) {
+    if (a->fused == WADG_STAGE_FUSED) {
       a->cur = 1 - a->cur;
       r = capture_step(a, dt);
       a->cur = 1 - a->cur;
@@ -497,7 +518,7 @@ int wadg_app_autotune(wadg_app *a, double dt, int nstages, int *warps, float *ti
 int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {
   if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
   const int fused = a->fused;
-  a->fused = 1;
+  a->fused = WADG_STAGE_FUSED;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -512,6 +533,34 @@ int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {
   a->fused = fused;
   if (r) return r;
   if (e != cudaSuccess) return afail(WADG_ERR_CUDA, "time_stage", e);
+  return WADG_OK;
+}
+
+int wadg_app_time_volsurf(wadg_app *a, double dt, int nstages, float *ms) {
+  if (!a || !ms || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
+  cudaEvent_t ev[3];
+  for (auto &x : ev) cudaEventCreate(&x);
+  float tot[2] = {0, 0};
+  int r = WADG_OK;
+  for (int s = 0; s < nstages && r == WADG_OK; ++s) {
+    cudaEventRecord(ev[0], a->stream);
+    r = volsurf(a);
+    cudaEventRecord(ev[1], a->stream);
+    if (!r) r = update(a, RK4A[s % 5], RK4B[s % 5], dt, a->curved);
+    cudaEventRecord(ev[2], a->stream);
+    cudaError_t e = cudaEventSynchronize(ev[2]);
+    if (e != cudaSuccess && !r) r = afail(WADG_ERR_CUDA, "time_volsurf", e);
+    if (!r)
+      for (int q = 0; q < 2; ++q) {
+        float t;
+        cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+        tot[q] += t;
+      }
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (r) return r;
+  ms[0] = tot[0];
+  ms[1] = tot[1];
   return WADG_OK;
 }
 

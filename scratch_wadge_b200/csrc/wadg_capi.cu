@@ -87,14 +87,16 @@ constexpr int volpairsW_cand(int i) {
   return i == 0 ? W0 : (W0 - 2 * i >= 2 ? W0 - 2 * i : 0);
 }
 
-template <int DIM, int N, bool CURVED, int W>
+// SURF: the volume + surface kernel (rhsQf unused; fgeo, mapPq read)
+template <int DIM, int N, bool CURVED, int W, bool SURF = false>
 int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
                        const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
                        const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
-                       const double *Qf, double *rhsQ, double *rhsQf) {
+                       const double *Qf, double *rhsQ, double *rhsQf,
+                       const double *fgeo = nullptr, const uint32_t *mapPq = nullptr) {
   using C = VolPairsCfg<DIM, N, CURVED, W>;
   static_assert(C::smem_vol <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
-  auto kern = vol_pairs_kernel<DIM, N, CURVED, W>;
+  auto kern = vol_pairs_kernel<DIM, N, CURVED, W, SURF>;
   static wadg_internal::PerDevice<bool> attr;
   if (!attr.here()) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_vol);
@@ -103,8 +105,20 @@ int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const doubl
   }
   const int grid = persistent_grid(K, C::E, C::smem_vol);
   kern<<<grid, C::threads, C::smem_vol, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
-                                                      VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys);
-  return after_launch("volume kernel");
+                                                      VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys, fgeo,
+                                                      mapPq);
+  return after_launch(SURF ? "volume + surface kernel" : "volume kernel");
+}
+
+// the volume + surface kernel, in the default CTA shape
+template <int DIM, int N, bool CURVED>
+int launch_volsurf(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
+                   const double *fgeo, const uint32_t *mapPq, const double *nrJ,
+                   const double *nsJ, const double *ntJ, const double *Drq, const double *Dsq,
+                   const double *Dtq, const double *VqLq, const double *VfPq, const double *Qf,
+                   double *rhsQ) {
+  return launch_vol_pairs_w<DIM, N, CURVED, volpairsW<DIM, N, CURVED>(), true>(
+      c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo, mapPq);
 }
 
 // the context's CTA shape (wadg_ctx_set_vol_warps), else the default
@@ -209,6 +223,9 @@ int kernel_shape(const wadg_ctx *c, int kernel, int K, int *E, int *grid) {
     case WADG_KERNEL_UPDATE:
       *E = UpdMmaCfg<DIM, N, CURVED>::EW;
       return update_grid<DIM, N, CURVED>(K, grid);
+    case WADG_KERNEL_VOLSURF:
+      vol_shape<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>(K, E, grid);
+      return WADG_OK;
     case WADG_KERNEL_ADJ_PAIRS:
       return wadg_internal::adj_pairs_shape(DIM, N, CURVED, K, E, grid);
     case WADG_KERNEL_STAGE: {
@@ -661,6 +678,41 @@ int wadg_euler_stage_3d(wadg_ctx *c, int K, int curved, const double *vgeo, cons
                                                         ntJ, Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq,
                                                         fa, fb, fdt, rhsQ_in, Qf_in, Q, resQ,
                                                         rhsQ_out, Qf_out)));
+}
+
+int wadg_euler_volsurf_3d(wadg_ctx *c, int K, int curved, const double *vgeo,
+                          const double *vfgeo, const double *fgeo, const uint32_t *mapPq,
+                          const double *nrJ, const double *nsJ, const double *ntJ,
+                          const double *Drq, const double *Dsq, const double *Dtq,
+                          const double *VqLq, const double *VfPq, const double *Qf, double *rhsQ) {
+  if (int r = check_ctx(c, 3, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ}) ||
+      (curved && !vfgeo))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  if (curved)
+    WADG_DISPATCH(c, return (launch_volsurf<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                           ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ)));
+  WADG_DISPATCH(c, return (launch_volsurf<D_, N_, false>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                          ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ)));
+}
+
+int wadg_euler_volsurf_2d(wadg_ctx *c, int K, int curved, const double *vgeo,
+                          const double *vfgeo, const double *fgeo, const uint32_t *mapPq,
+                          const double *nrJ, const double *nsJ, const double *Drq,
+                          const double *Dsq, const double *VqLq, const double *VfPq,
+                          const double *Qf, double *rhsQ) {
+  if (int r = check_ctx(c, 2, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (any_null({vgeo, fgeo, mapPq, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, Qf, rhsQ}) || (curved && !vfgeo))
+    return fail(WADG_ERR_INVALID, "null pointer argument");
+  if (curved)
+    WADG_DISPATCH(c, return (launch_volsurf<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                           nullptr, Drq, Dsq, nullptr, VqLq, VfPq,
+                                                           Qf, rhsQ)));
+  WADG_DISPATCH(c, return (launch_volsurf<D_, N_, false>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
+                                                          nullptr, Drq, Dsq, nullptr, VqLq, VfPq,
+                                                          Qf, rhsQ)));
 }
 
 int wadg_euler_stage_2d(wadg_ctx *c, int K, int curved, const double *vgeo, const double *vfgeo,

@@ -348,6 +348,43 @@ __device__ __forceinline__ void ecflux_n_nolog(const NodeState<DIM> &a, const No
   F[DIM + 1] = f4 * un;
 }
 
+// sqrt(x) for x >= 0 (0 for x <= 0): the reciprocal square root estimate
+// rsqrt.approx.f64 refined by two Newton-Raphson steps on y^-2 = x, then one
+// Newton step on s^2 = x for s = x y; a few ulp, for the surface kernels'
+// wave speeds (which only enter the penalty's max)
+__device__ __forceinline__ double fsqrt(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = y * fma(-0.5 * x * y, y, 1.5);
+  y = y * fma(-0.5 * x * y, y, 1.5);
+  double s = x * y;
+  s = fma(0.5 * y, fma(-s, s, x), s);
+  return x > 0.0 ? s : 0.0;
+}
+
+// node state of a conservative trace without the logarithms (for
+// ecflux_n_nolog), with |u|^2 and the squared sound speed gamma p / rho of the
+// surface penalty; reciprocals (rcp) in place of divisions
+template <int DIM>
+__device__ __forceinline__ NodeState<DIM> node_state_surf(const double *q, int stride, const Phys &P,
+                                                          double &kin, double &c2) {
+  NodeState<DIM> s;
+  s.rho = q[0];
+  const double ir = rcp(s.rho);
+  kin = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.vel[d] = q[(1 + d) * stride] * ir;
+    kin = fma(s.vel[d], s.vel[d], kin);
+  }
+  const double p = P.gm1 * (q[(DIM + 1) * stride] - 0.5 * s.rho * kin);
+  s.beta = 0.5 * s.rho * rcp(p);
+  c2 = P.gamma * p * ir;
+  s.lrho = 0.0;
+  s.lbeta = 0.0;
+  return s;
+}
+
 // node state without the logarithms (for ecflux_n_nolog)
 template <int DIM>
 __device__ __forceinline__ NodeState<DIM> node_state_nolog(const double *q, int stride, const Phys &P) {

@@ -77,9 +77,9 @@ int wadg_ensemble_create(int nbins, wadg_app **bins, wadg_ensemble **out) {
   *out = nullptr;
   wadg_ensemble *s = new wadg_ensemble;
   s->bins.assign(bins, bins + nbins);
-  s->fused = wadg_app_get_fused(bins[0]);
+  s->fused = wadg_app_get_fused(bins[0]) == WADG_STAGE_FUSED;
   for (auto *a : s->bins) {
-    if (!a || wadg_app_get_fused(a) != s->fused) {
+    if (!a || (wadg_app_get_fused(a) == WADG_STAGE_FUSED) != s->fused) {
       delete s;
       return efail(WADG_ERR_INVALID, "bins must be non-null and share the stage variant");
     }

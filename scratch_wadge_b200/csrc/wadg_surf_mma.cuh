@@ -70,21 +70,14 @@ surf_mma_kernel(int K, const double *__restrict__ fgeo, const uint32_t *__restri
         UM[f] = Qf[idM + f * NF];
         UP[f] = Qf[idP + f * NF];
       }
-      const NodeState<DIM> M = node_state_nolog<DIM>(UM, 1, P);
-      const NodeState<DIM> Pp = node_state_nolog<DIM>(UP, 1, P);
+      double kM, kP, c2M, c2P;
+      const NodeState<DIM> M = node_state_surf<DIM>(UM, 1, P, kM, c2M);
+      const NodeState<DIM> Pp = node_state_surf<DIM>(UP, 1, P, kP, c2P);
       double F[Nf];
       ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
       // wave speeds |u| + sqrt(gamma p / rho)
-      double kM = 0.0, kP = 0.0;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        kM = fma(M.vel[d], M.vel[d], kM);
-        kP = fma(Pp.vel[d], Pp.vel[d], kP);
-      }
-      const double pM = P.gm1 * (UM[Nf - 1] - 0.5 * M.rho * kM);
-      const double pP = P.gm1 * (UP[Nf - 1] - 0.5 * Pp.rho * kP);
-      const double lamM = sqrt(kM) + sqrt(P.gamma * pM / M.rho);
-      const double lamP = sqrt(kP) + sqrt(P.gamma * pP / Pp.rho);
+      const double lamM = fsqrt(kM) + fsqrt(c2M);
+      const double lamP = fsqrt(kP) + fsqrt(c2P);
       const double tau = (DIM == 3) ? P.tau : 1.0;
       const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
       const double *rf = rhsQf + idM;

@@ -306,6 +306,80 @@ struct VolPairs {
     }
   }
 
+  // surface flux + Lax-Friedrichs penalty at the face points of the group's
+  // batch elements [e0, e0 + G) (the TS threads t0, t0 + TS, ... of the
+  // group), added to the face-row accumulators: sf = rhsQf + 1/2
+  // F_S(u-, u+).nJ - tau/4 max(lam-, lam+) sJ (u+ - u-) (Euler3D.okl:3256-3346,
+  // Euler2D.okl:1373-1453).  The minus state is the pair phase's node state
+  // (velocity stored halved) and the trace in uf; the plus trace is gathered
+  // from uf through mapPq (the neighbour indices of all of a thread's face
+  // points are loaded first).
+  template <int TS>
+  __device__ __forceinline__ void surface(int K, int k0, int e0, int t0,
+                                          const double *__restrict__ fgeo,
+                                          const uint32_t *__restrict__ mapPq,
+                                          const double *__restrict__ uf, const Phys &P) const {
+    constexpr int NFG = El::Nfgeo, NPT = (G * NF + TS - 1) / TS;
+    uint32_t idP[NPT];
+#pragma unroll
+    for (int u = 0; u < NPT; ++u) {
+      const int t = t0 + u * TS, k = k0 + e0 + t / NF;
+      idP[u] = (t < G * NF && k < K) ? mapPq[t % NF + (size_t)k * NF] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < NPT; ++u) {
+      const int t = t0 + u * TS;
+      const int ee = e0 + t / NF, f = t % NF, k = k0 + ee;
+      if (t >= G * NF || k >= K) continue;
+      const size_t idM = f + (size_t)k * NF * Nf;
+      const double *fg = fgeo + (size_t)k * NF * NFG + f;
+      double nJ[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) nJ[d] = fg[d * NF];
+      const double sJ = fg[DIM * NF];
+      double UM[Nf], UP[Nf];
+#pragma unroll
+      for (int q = 0; q < Nf; ++q) {
+        UM[q] = uf[idM + q * NF];
+        UP[q] = uf[idP[u] + q * NF];
+      }
+      NodeState<DIM> M = load(sSt + ee * SE, Nq + f);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) M.vel[d] *= 2.0;  // the pair phase's states hold u/2
+      double kM, kP, c2M, c2P;
+      node_state_surf<DIM>(UM, 1, P, kM, c2M);
+      const NodeState<DIM> Pp = node_state_surf<DIM>(UP, 1, P, kP, c2P);
+      double F[Nf];
+      ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
+      const double lamM = fsqrt(kM) + fsqrt(c2M);
+      const double lamP = fsqrt(kP) + fsqrt(c2P);
+      const double tau = (DIM == 3) ? P.tau : 1.0;
+      const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
+      double *a0 = sAcc + ee * SA;
+#pragma unroll
+      for (int q = 0; q < Nf; ++q) a0[q * NF + f] = a0[q * NF + f] + 0.5 * F[q] - Lfc * (UP[q] - UM[q]);
+    }
+  }
+
+  // lift: rows += VqLq sf on the rotated weights (VqLq = 2 W1), the warps of
+  // the group splitting the face nodes as in the pair phase
+  __device__ __forceinline__ void lift(double (&acc)[R][Nf]) const {
+    const double *sf = sAcc + e * SA;
+    const int nfh = T::nf(h), f0h = T::f0(h);
+    const double *w1h = sW1 + R * L * f0h;
+    for (int s = 0; s < nfh; ++s) {
+      int ff = l + s;
+      if (ff >= nfh) ff -= nfh;
+      const int f = f0h + ff;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double w = 2.0 * w1h[(r * nfh + s) * L + l];
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) acc[r][q] = fma(w, sf[q * NF + f], acc[r][q]);
+      }
+    }
+  }
+
   // warp 1 parks its partial rows in element e's state block ([Nf][Nq]);
   // call between two __syncthreads
   __device__ __forceinline__ void park_rows(const double (&acc)[R][Nf]) const {
@@ -323,7 +397,14 @@ struct VolPairs {
   }
 };
 
-template <int DIM, int N, bool CURVED, int W>
+// SURF = false: the volume kernel (euler_vol_*): rhsQ <- the volume rows,
+// rhsQf <- the face rows.  SURF = true: the volume and the surface kernel of
+// a stage in one launch: after the pairs, the group adds the surface flux and
+// penalty to its face rows (gathering the neighbours' traces from Qf through
+// mapPq; Qf is only read, so every element's traces are final) and lifts
+// them into its rows; rhsQ <- the whole right-hand side the surface kernel
+// would leave, rhsQf is not written (fgeo and mapPq unused when false)
+template <int DIM, int N, bool CURVED, int W, bool SURF = false>
 __global__ void __launch_bounds__(32 * W, 1)
 vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
                  const double *__restrict__ nrJ, const double *__restrict__ nsJ,
@@ -331,7 +412,8 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
                  const double *__restrict__ Dsq, const double *__restrict__ Dtq,
                  const double *__restrict__ VqLq, const double *__restrict__ VfPq,
                  const double *__restrict__ Qf, double *__restrict__ rhsQ,
-                 double *__restrict__ rhsQf, Phys P) {
+                 double *__restrict__ rhsQf, Phys P, const double *__restrict__ fgeo = nullptr,
+                 const uint32_t *__restrict__ mapPq = nullptr) {
   using V = VolPairs<DIM, N, CURVED, W>;
   constexpr int Nq = V::Nq, NF = V::NF, Nf = V::Nf, R = V::R, L = V::L, E = V::E, H = V::H;
   extern __shared__ double smem[];
@@ -378,6 +460,11 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     double acc[R][Nf];
     v.pairs(acc, P);
     gsync();  // the group's pairs done: its state block becomes the row buffer
+    if (SURF) {
+      v.template surface<GT>(K, k0, q * G, tq, fgeo, mapPq, Qf, P);
+      gsync();  // face rows complete (and the states read): lift, then park
+      v.lift(acc);
+    }
     v.park_rows(acc);
     gsync();
     const int k = k0 + v.e;
@@ -394,9 +481,11 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           }
         }
       }
-      const double *a0 = v.sAcc + v.e * V::SA;
-      double *outf = rhsQf + (size_t)k * NF * Nf;
-      for (int t = v.h * L + v.l; t < NF * Nf; t += H * L) outf[t] = a0[t];
+      if (!SURF) {
+        const double *a0 = v.sAcc + v.e * V::SA;
+        double *outf = rhsQf + (size_t)k * NF * Nf;
+        for (int t = v.h * L + v.l; t < NF * Nf; t += H * L) outf[t] = a0[t];
+      }
     }
   }
 }
@@ -453,67 +542,10 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
     gsync();
 
     // ---- surface: sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam) sJ (u+ - u-)
-    // (Euler3D.okl:3256-3346, Euler2D.okl:1373-1453); stored over the face
-    // accumulators
-    for (int t = tid; t < G * NF; t += nth) {
-      const int ee = e0 + t / NF, f = t % NF, k = k0 + ee;
-      if (k >= K) continue;
-      const size_t idM = f + (size_t)k * NF * Nf;
-      const size_t idP = mapPq[f + (size_t)k * NF];
-      const double *fg = fgeo + (size_t)k * NF * NFG + f;
-      double nJ[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) nJ[d] = fg[d * NF];
-      const double sJ = fg[DIM * NF];
-      double UM[Nf], UP[Nf];
-#pragma unroll
-      for (int q = 0; q < Nf; ++q) {
-        UM[q] = uf[idM + q * NF];
-        UP[q] = uf[idP + q * NF];
-      }
-      NodeState<DIM> M = v.load(v.sSt + ee * SE, Nq + f);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) M.vel[d] *= 2.0;  // the pair phase's states hold u/2
-      const NodeState<DIM> Pp = node_state_nolog<DIM>(UP, 1, P);
-      double F[Nf];
-      ecflux_n_nolog<DIM>(M, Pp, nJ, P, F);
-      double kM = 0.0, kP = 0.0;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        const double um = UM[1 + d] / UM[0], up = UP[1 + d] / UP[0];
-        kM = fma(um, um, kM);
-        kP = fma(up, up, kP);
-      }
-      const double pM = P.gm1 * (UM[Nf - 1] - 0.5 * UM[0] * kM);
-      const double pP = P.gm1 * (UP[Nf - 1] - 0.5 * UP[0] * kP);
-      const double lamM = sqrt(kM) + sqrt(P.gamma * pM / UM[0]);
-      const double lamP = sqrt(kP) + sqrt(P.gamma * pP / UP[0]);
-      const double tau = (DIM == 3) ? P.tau : 1.0;
-      const double Lfc = tau * 0.25 * fmax(lamM, lamP) * sJ;
-      double *a0 = v.sAcc + ee * SA;
-#pragma unroll
-      for (int q = 0; q < Nf; ++q) a0[q * NF + f] = a0[q * NF + f] + 0.5 * F[q] - Lfc * (UP[q] - UM[q]);
-    }
+    // over the face accumulators, then the lift rows += VqLq sfS
+    v.template surface<GT>(K, k0, e0, tid, fgeo, mapPq, uf, P);
     gsync();
-
-    // ---- lift: rows += VqLq sfS, on the rotated weights (VqLq = 2 W1),
-    // the two warps splitting the face nodes as in the pair phase
-    {
-      const double *sf = v.sAcc + v.e * SA;
-      const int nfh = V::T::nf(v.h), f0h = V::T::f0(v.h);
-      const double *w1h = v.sW1 + R * L * f0h;
-      for (int s = 0; s < nfh; ++s) {
-        int ff = v.l + s;
-        if (ff >= nfh) ff -= nfh;
-        const int f = f0h + ff;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const double w = 2.0 * w1h[(r * nfh + s) * L + v.l];
-#pragma unroll
-          for (int q = 0; q < Nf; ++q) acc[r][q] = fma(w, sf[q * NF + f], acc[r][q]);
-        }
-      }
-    }
+    v.lift(acc);
     v.park_rows(acc);  // the state block is free after the surface phase
     gsync();
     if (v.h == 0) {

@@ -65,3 +65,12 @@ def stage_flops_per_element(dim, Nq, NfqNf, curved, series=True):
     vf = PAIR_FLOPS[(dim, bool(curved), bool(series))][1]
     mm = 2 * Nf * (Nq * NfqNf + (Nq * Nq * (4 if curved else 2)) + NfqNf * Nq)
     return vol_flops_per_element(dim, Nq, NfqNf, curved, series) + NfqNf * vf + mm
+
+
+def volsurf_flops_per_element(dim, Nq, NfqNf, curved, series=True):
+    """Algorithmic flops of the volume + surface kernel per element: the
+    volume pairs, the surface flux (one face-volume pair's count per face
+    node) and the lift VqLq*sf (2 flops per multiply-add)."""
+    Nf = dim + 2
+    vf = PAIR_FLOPS[(dim, bool(curved), bool(series))][1]
+    return vol_flops_per_element(dim, Nq, NfqNf, curved, series) + NfqNf * vf + 2 * Nf * Nq * NfqNf

@@ -1,7 +1,7 @@
 """The persistent kernels over several batches per CTA, against the oracle.
 
-The volume, update and fused stage kernels (and the adjoint's pair VJP
-kernel) launch at most as many CTAs as are resident at once; CTA b then takes
+The volume, volume + surface, update and fused stage kernels (and the
+adjoint's pair VJP kernel) launch at most as many CTAs as are resident at once; CTA b then takes
 batches b, b + grid, b + 2 grid, ...  Small meshes never leave the first
 batch, so each case here takes the kernel's own launch shape
 (wadg_kernel_shape) and runs it on K = 2 * grid * E + r elements with
@@ -92,9 +92,10 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     sh = shapes(ctx, curved, big)
     Ku_E, Ku_g = ctx.shape("update", curved, big)
     Ks_E, Ks_g = ctx.shape("stage", curved, big)
+    Kvs_E, Kvs_g = ctx.shape("volsurf", curved, big)
     Kvol = {w: multibatch_K(E, g) for w, E, g in sh}
-    Kupd, Kst = multibatch_K(Ku_E, Ku_g), multibatch_K(Ks_E, Ks_g)
-    mesh = mesh_with_at_least(dim, curved, max(max(Kvol.values()), Kupd, Kst))
+    Kupd, Kst, Kvs = multibatch_K(Ku_E, Ku_g), multibatch_K(Ks_E, Ks_g), multibatch_K(Kvs_E, Kvs_g)
+    mesh = mesh_with_at_least(dim, curved, max(max(Kvol.values()), Kupd, Kst, Kvs))
     geo = build_geometry_gpu(mesh, N)
     d = Dev(cuda, geo, curved)
     ref = oracle(ops, curved)
@@ -144,6 +145,23 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
         assert np.isfinite(a[k]).all(), k
         assert rel(h[k][:K], a[k]) < RTOL, (k, rel(h[k][:K], a[k]))
         assert np.array_equal(h[k][K:], st[k][K:]), k
+
+    # volume + surface kernel over Kvs elements (gathers traces past K)
+    K = Kvs
+    s = d.put(st)
+    d.ctx.volsurf(curved, K, *[d.g[n].data_ptr() for n in ("vgeo", "vfgeo", "fgeo", "mapPq", "nrJ", "nsJ",
+                                                           "ntJ", "Drq", "Dsq", "Dtq", "VqLq", "VfPq")],
+                  s["Qf"].data_ptr(), s["rhsQ"].data_ptr())
+    d.sync()
+    h = d.get(s)
+    a = _first(st, K)
+    a["rhsQf"][:] = 0.0
+    ref.vol(geo, a["Qf"], a["rhsQ"], a["rhsQf"])
+    ref.surf(geo, np.ascontiguousarray(st["Qf"]).copy(), a["rhsQf"], a["rhsQ"])
+    assert np.isfinite(a["rhsQ"]).all()
+    assert rel(h["rhsQ"][:K], a["rhsQ"]) < RTOL, rel(h["rhsQ"][:K], a["rhsQ"])
+    assert np.array_equal(h["rhsQ"][K:], st["rhsQ"][K:])
+    assert np.array_equal(h["Qf"], st["Qf"])
 
     # fused stage kernel over Kst elements (reads the state, writes new buffers)
     K = Kst

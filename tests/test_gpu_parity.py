@@ -73,6 +73,14 @@ class Dev:
                        s["Qf"].data_ptr(), s["Q"].data_ptr(), s["resQ"].data_ptr(),
                        out["rhsQ"].data_ptr(), out["Qf"].data_ptr())
 
+    def volsurf(self, s):
+        g = self.g
+        self.ctx.volsurf(self.curved, self.geo.K, g["vgeo"].data_ptr(), g["vfgeo"].data_ptr(),
+                         g["fgeo"].data_ptr(), g["mapPq"].data_ptr(), g["nrJ"].data_ptr(),
+                         g["nsJ"].data_ptr(), g["ntJ"].data_ptr(), g["Drq"].data_ptr(), g["Dsq"].data_ptr(),
+                         g["Dtq"].data_ptr(), g["VqLq"].data_ptr(), g["VfPq"].data_ptr(),
+                         s["Qf"].data_ptr(), s["rhsQ"].data_ptr())
+
     def sync(self):
         self.torch.cuda.synchronize()
 
@@ -137,6 +145,30 @@ def test_fused_stage_matches_reference_golden(cuda, name):
         assert rel(got[k], c.z["upd_" + k]) < RTOL, (k, rel(got[k], c.z["upd_" + k]))
     # the inputs are untouched
     assert np.array_equal(s["rhsQ"].cpu().numpy(), c.z["in_rhsQ"])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_volsurf_matches_reference_golden(cuda, name):
+    """wadg_euler_volsurf_*: the volume and surface kernels in one launch
+    leave the reference's right-hand side after its surface kernel"""
+    c = Case(name)
+    d = Dev(cuda, c.geo, c.curved)
+    s = d.put(c.state())
+    d.volsurf(s)
+    d.sync()
+    assert rel(s["rhsQ"].cpu().numpy(), c.z["surf_rhsQ"]) < RTOL
+    assert np.array_equal(s["Qf"].cpu().numpy(), c.z["in_Qf"])  # traces only read
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_app_volsurf_variant_matches_reference_step(cuda, name):
+    c = Case(name)
+    app = capi.App(c.geo, c.curved)
+    app.set_stage_variant("volsurf")
+    st = c.state()
+    app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
+    app.rk_run(c.dt, 1, graph=True)
+    assert rel(app.get_state()["Q"], c.z["step_Q"]) < RTOL
 
 
 def test_fused_stage_rejects_aliasing(cuda):
