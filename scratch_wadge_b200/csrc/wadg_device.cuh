@@ -148,7 +148,7 @@ template <int DIM>
 __device__ __forceinline__ NodeState<DIM> node_state(const double *q, int stride, const Phys &P) {
   NodeState<DIM> s;
   s.rho = q[0];
-  const double ir = 1.0 / s.rho;
+  const double ir = rcp(s.rho);
   double kin = 0.0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
@@ -157,7 +157,7 @@ __device__ __forceinline__ NodeState<DIM> node_state(const double *q, int stride
   }
   const double E = q[(DIM + 1) * stride];
   const double p = P.gm1 * (E - 0.5 * s.rho * kin);
-  s.beta = s.rho / (2.0 * p);
+  s.beta = 0.5 * s.rho * rcp(p);
   s.lrho = log(s.rho);
   s.lbeta = log(s.beta);
   return s;
@@ -200,10 +200,10 @@ __device__ __forceinline__ void VU(const double *U, double *V, const Phys &P) {
   double m2 = 0.0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) m2 = fma(U[1 + d], U[1 + d], m2);
-  const double rhoe = E - 0.5 * m2 / rho;
+  const double rhoe = E - 0.5 * m2 * rcp(rho);
   // s = log((gamma-1) rhoe / rho^gamma), written with two logarithms
   const double s = log(P.gm1 * rhoe) - P.gamma * log(rho);
-  const double irhoe = 1.0 / rhoe;
+  const double irhoe = rcp(rhoe);
   V[0] = (-E + rhoe * (P.gamma + 1.0 - s)) * irhoe;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) V[1 + d] = U[1 + d] * irhoe;
@@ -217,14 +217,15 @@ __device__ __forceinline__ void UV(const double *V, double *U, const Phys &P) {
   double vv = 0.0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) vv = fma(V[1 + d], V[1 + d], vv);
-  const double sV = P.gamma - V[0] + vv / (2.0 * Vl);
+  const double h = 0.5 * vv * rcp(Vl);  // vv / (2 V_l)
+  const double sV = P.gamma - V[0] + h;
   // rhoe = ((gamma-1)/(-V_l)^gamma)^(1/(gamma-1)) exp(-sV/(gamma-1)), as one
   // exponential: exp((log(gamma-1) - gamma log(-V_l) - sV) / (gamma-1))
   const double rhoe = exp((P.lgm1 - P.gamma * log(-Vl) - sV) * P.igm1);
   U[0] = -rhoe * Vl;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) U[1 + d] = rhoe * V[1 + d];
-  U[DIM + 1] = rhoe * (1.0 - vv / (2.0 * Vl));
+  U[DIM + 1] = rhoe * (1.0 - h);
 }
 
 }  // namespace wadg

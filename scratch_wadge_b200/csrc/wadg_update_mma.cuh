@@ -130,9 +130,9 @@ __device__ __forceinline__ void mtile_store(double *Y, int mt, int lane, const d
   for (int i = 0; i < 2; ++i) {
     const int e = 2 * (lane & 3) + i;
     const bool ok = e < ne;
-    const double J = (DIVJ && ok) ? Jq[(size_t)(k0 + e) * Nq + m] : 1.0;
+    const double cJ = (DIVJ && ok) ? c * rcp(Jq[(size_t)(k0 + e) * Nq + m]) : 1.0;
 #pragma unroll
-    for (int f = 0; f < Nf; ++f) Y[m * LD + f * 8 + e] = ok ? (DIVJ ? c * D[f][i] / J : D[f][i]) : 0.0;
+    for (int f = 0; f < Nf; ++f) Y[m * LD + f * 8 + e] = ok ? (DIVJ ? cJ * D[f][i] : D[f][i]) : 0.0;
   }
 }
 
@@ -204,10 +204,11 @@ __device__ __forceinline__ void update_group(
       for (int i = 0; i < 2; ++i) {
         const int e = 2 * (lane & 3) + i;
         const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
+        const double m2J = CURVED ? 0.0 : -2.0 * rcp(Jv[i]);  // -2 / J
         double U[Nf], V[Nf];
 #pragma unroll
         for (int f = 0; f < Nf; ++f) {
-          const double r = CURVED ? D[f][i] : -2.0 * D[f][i] / Jv[i];
+          const double r = CURVED ? D[f][i] : m2J * D[f][i];
           const double res = fa * res0[i][f] + fdt * r;
           U[f] = q0[i][f] + fb * res;
           if (ev[i]) {
