@@ -279,6 +279,63 @@ __device__ __forceinline__ void ecflux_n_warp(const NodeState<DIM> &a, const Nod
   F[DIM + 1] = f4 * un;
 }
 
+// ecflux_n_warp_h for R row states a[r] against one column state b: one
+// warp vote for all R pairs of every lane (the u^2 series when all of them
+// have u < 1e-6), then the R fluxes side by side -- independent chains in one
+// basic block, which the scheduler interleaves.  Same value per pair as
+// ecflux_n_warp_h to rounding.  Must be called by all 32 lanes of the warp.
+template <int DIM, int R>
+__device__ __forceinline__ void ecflux_n_warp_hR(const NodeState<DIM> (&a)[R], const NodeState<DIM> &b,
+                                                 const double (&n)[R][DIM], const Phys &P,
+                                                 double (&F)[R][DIM + 2]) {
+  double hsr[R], dr[R], db[R], isb[R], ur[R], ub[R];
+  bool small = true;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const double sr = a[r].rho + b.rho, sb = a[r].beta + b.beta;
+    dr[r] = a[r].rho - b.rho;
+    db[r] = a[r].beta - b.beta;
+    const double isr = rcp1(sr);
+    isb[r] = rcp(sb);
+    const double fr = dr[r] * isr, fb = db[r] * isb[r];
+    ur[r] = fr * fr;
+    ub[r] = fb * fb;
+    hsr[r] = 0.5 * sr;
+    small = small && fmax(ur[r], ub[r]) < 1e-6;
+  }
+  double rl[R], ibl[R];
+  if (__all_sync(0xffffffffu, small)) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      rl[r] = hsr[r] * polyG2(ur[r]);
+      ibl[r] = 2.0 * isb[r] * polyF2(ub[r]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      rl[r] = (ur[r] < 1e-2) ? hsr[r] * polyG(ur[r]) : dr[r] * rcp(a[r].lrho - b.lrho);
+      ibl[r] = (ub[r] < 1e-2) ? 2.0 * isb[r] * polyF(ub[r]) : (a[r].lbeta - b.lbeta) * rcp(db[r]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const double pa = hsr[r] * isb[r];
+    double ubar[DIM], un = 0.0, hv = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      ubar[d] = a[r].vel[d] + b.vel[d];
+      un = fma(ubar[d], n[r][d], un);
+      hv = fma(a[r].vel[d], b.vel[d], hv);
+    }
+    const double f4 = fma(rl[r], fma(ibl[r], P.cbeta, 2.0 * hv), pa);
+    const double F0 = rl[r] * un;
+    F[r][0] = F0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) F[r][1 + d] = fma(F0, ubar[d], pa * n[r][d]);
+    F[r][DIM + 1] = f4 * un;
+  }
+}
+
 // ecflux_n_warp for states whose velocity is stored halved (vel = u/2), the
 // pair kernel's layout: ubar = a.vel + b.vel, (ua.ub)/2 = 2 (a.vel . b.vel),
 // and (rho_a + rho_b)/2 is formed once for rholog and pa.  Same value to

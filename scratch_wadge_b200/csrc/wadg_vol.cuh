@@ -236,10 +236,11 @@ struct VolPairs {
     const int j0 = (H == 2 && h) ? Nq / 2 : 0, j1 = (H == 2 && !h) ? Nq / 2 : Nq;
     for (int j = j0; j < j1; ++j) {
       const NodeState<DIM> B = load(st, j);
+      double nv[R][DIM], F[R][Nf];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int i = ir[r];
-        double rr[DIM], nv[DIM], F[Nf];
+        double rr[DIM];
 #pragma unroll
         for (int a = 0; a < DIM; ++a) rr[a] = sD[a * Nq * Nq + i + j * Nq];
 #pragma unroll
@@ -251,12 +252,14 @@ struct VolPairs {
                                       : Ge[a * DIM + d];
             v = fma(gad, rr[a], v);
           }
-          nv[d] = v;
+          nv[r][d] = v;
         }
-        ecflux_n_warp_h<DIM>(A[r], B, nv, P, F);
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) acc[r][q] += F[q];
       }
+      ecflux_n_warp_hR<DIM, R>(A, B, nv, P, F);
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int q = 0; q < Nf; ++q) acc[r][q] += F[r][q];
     }
 
     // volume-face pairs, each evaluated once: warp h takes its face nodes
@@ -276,6 +279,7 @@ struct VolPairs {
       double af[Nf];
 #pragma unroll
       for (int q = 0; q < Nf; ++q) af[q] = 0.0;
+      double nvr[R][DIM], F[R][Nf];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if (CURVED) {
@@ -287,17 +291,22 @@ struct VolPairs {
             for (int a = 0; a < DIM; ++a)
               v = fma(st[(NS + a * DIM + d) * NN + i] + st[(NS + a * DIM + d) * NN + Nq + f],
                       sNr[fc * DIM + a], v);
-            nv[d] = v;
+            nvr[r][d] = v;
           }
+        } else {
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) nvr[r][d] = nv[d];
         }
-        double F[Nf];
-        ecflux_n_warp_h<DIM>(A[r], B, nv, P, F);
+      }
+      ecflux_n_warp_hR<DIM, R>(A, B, nvr, P, F);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
         const double w1 = w1h[(r * nfh + s) * L + l];
         const double w2 = w2h[(r * nfh + s) * L + l];
 #pragma unroll
         for (int q = 0; q < Nf; ++q) {
-          acc[r][q] = fma(w1, F[q], acc[r][q]);
-          af[q] = fma(w2, F[q], af[q]);
+          acc[r][q] = fma(w1, F[r][q], acc[r][q]);
+          af[q] = fma(w2, F[r][q], af[q]);
         }
       }
 #pragma unroll
