@@ -1,9 +1,11 @@
 """Reference-element operators for the entropy-stable DG right-hand side.
 
 ``load(dim, N)`` returns the operator tables of the reference element of degree
-N (cubature degree 2N), exactly as the reference's host builder produces them
+N (cubature degree 2N), as the reference's host builder produces them
 (build_ref_ops_2D/3D in operators.cpp:104-341 and the hybridized operators of
-host_operators_new_2D/3D, operators_c.cpp:46-69, 212-241):
+host_operators_new_2D/3D, operators_c.cpp:46-69, 212-241), built by
+refbuild.py from the node and cubature point sets in
+data/points_<dim>d_N<N>.npz:
 
   nodes r,s,t (Np); volume cubature rq,sq,tq,wq (Nq); face cubature
   rfq,sfq,tfq,wfq and reference normals nrJ,nsJ,ntJ (Nfq*Nfaces, face-major);
@@ -11,12 +13,12 @@ host_operators_new_2D/3D, operators_c.cpp:46-69, 212-241):
   VqLq (Nq x NfqNf); VqPq (Nq x Nq); VfPq (NfqNf x Nq);
   Drq, Dsq, Dtq (Nq x Nq) = Vq D Pq - 1/2 Vq Lq diag(n) Vfq Pq.
 
-The tables live in data/refops_<dim>d_N<N>.npz (generated from the reference
-builder by tests/golden/gen_refops.py).  This module also restates the
-orthonormal simplex basis (Hesthaven & Warburton, "Nodal Discontinuous Galerkin
-Methods", 2008, App. A; the same construction as operators.cpp's
-Vandermonde2D/3D) to build interpolation matrices between node sets of
-different degree, which the curved geometry builder needs.
+The reference builder's own tables (tests/golden/refops/, made by
+tests/golden/gen_refops.py) pin the built ones in tests/test_refbuild.py.
+This module also holds the orthonormal simplex basis (Hesthaven & Warburton,
+"Nodal Discontinuous Galerkin Methods", 2008, App. A; the same construction
+as operators.cpp's Vandermonde2D/3D), which the builder and the interpolation
+between node sets of different degree (curved geometry) use.
 """
 
 from __future__ import annotations
@@ -50,11 +52,8 @@ class RefOps:
 
 @functools.lru_cache(maxsize=None)
 def load(dim: int, N: int) -> RefOps:
-    path = os.path.join(DATA, f"refops_{dim}d_N{N}.npz")
-    if not os.path.exists(path):
-        raise ValueError(f"no operator table for dim={dim} N={N} ({path})")
-    with np.load(path) as z:
-        return RefOps({k: z[k] for k in z.files})
+    from . import refbuild
+    return RefOps(refbuild.build(dim, N))
 
 
 # ----------------------------------------------------------- simplex basis

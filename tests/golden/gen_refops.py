@@ -1,15 +1,17 @@
-"""Generate the reference-element operator tables shipped in
-scratch_wadge_b200/data/refops_<dim>d_N<N>.npz.
-
-The tables are outputs of the reference's own operator builder
+"""Generate, from the reference's own operator builder
 (build_ref_ops_2D/3D, operators.cpp:104-341, and the hybridized operators of
-host_operators_new_2D/3D, operators_c.cpp:46-69, 212-241), compiled from the
-reference sources by oracle/build.py.  They are the inputs the reference's
-kernels receive (Drq, Dsq, Dtq, VqLq, VqPq, VfPq, nrJ, ...) together with the
-node, cubature and interpolation data the host geometry builder needs.  They
-hold the quadrature rules tabulated in the reference's node_data.h as the
-reference's builder consumes them, so the GPU path sees exactly the
-reference's operators.
+host_operators_new_2D/3D, operators_c.cpp:46-69, 212-241, compiled from the
+reference sources by oracle/build.py):
+
+* tests/golden/refops/refops_<dim>d_N<N>.npz -- every table of the reference
+  element (the inputs the reference's kernels receive: Drq, Dsq, Dtq, VqLq,
+  VqPq, VfPq, nrJ, ...; and V, Dr, Vq, Pq, Vfq, ...), the check that
+  tests/test_refbuild.py pins scratch_wadge_b200/refbuild.py against;
+* scratch_wadge_b200/data/points_<dim>d_N<N>.npz -- the point sets those
+  tables are built from: the interpolation nodes, the volume cubature and,
+  in 3D, the triangle cubature of the faces, as tabulated in the
+  reference's node_data.h and read by its builder.  refbuild.py builds the
+  product's operators from these.
 
 Run once in a checkout where the reference tree exists:
     python tests/golden/gen_refops.py
@@ -68,13 +70,21 @@ def refelem(dim, N, M=None):
 def main():
     if not build.reference_present():
         raise SystemExit("reference tree not found")
-    outdir = os.path.join(ROOT, "scratch_wadge_b200", "data")
-    os.makedirs(outdir, exist_ok=True)
+    checkdir = os.path.join(ROOT, "tests", "golden", "refops")
+    ptsdir = os.path.join(ROOT, "scratch_wadge_b200", "data")
+    os.makedirs(checkdir, exist_ok=True)
+    os.makedirs(ptsdir, exist_ok=True)
     for dim, degs in ((2, (1, 2, 3, 4, 5)), (3, (1, 2, 3, 4, 5))):
         for N in degs:
             d = refelem(dim, N)
-            path = os.path.join(outdir, f"refops_{dim}d_N{N}.npz")
+            path = os.path.join(checkdir, f"refops_{dim}d_N{N}.npz")
             np.savez_compressed(path, **d)
+            Nfq = int(d["sizes"][5])
+            pts = dict(r=d["r"], s=d["s"], rq=d["rq"], sq=d["sq"], wq=d["wq"])
+            if dim == 3:
+                pts.update(t=d["t"], tq=d["tq"], ref_rfq=d["ref_rfq"], ref_sfq=d["ref_sfq"],
+                           wtri=d["wfq"][:Nfq])
+            np.savez_compressed(os.path.join(ptsdir, f"points_{dim}d_N{N}.npz"), **pts)
             print(path, d["sizes"].tolist())
 
 

