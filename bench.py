@@ -15,8 +15,8 @@ fused stage kernel (wadg_euler_stage_3d: vol + surf + update in one launch per
 stage), whichever is faster on this GPU (both are timed, `stage_variant`),
 replayed as a CUDA graph; the line also reports the three kernels timed one by
 one (`roofline`, `hbm_kernels`).  Two more workloads are reported beside the
-headline: `ensemble` (256 independent 2D vortex solves, batched against one
-solver per instance) and `adjoint` (the checkpointed discrete adjoint of a
+headline: `ensemble` (256 independent 2D vortex solves to a final time, each
+with its own step, batched against one solver per instance) and `adjoint` (the checkpointed discrete adjoint of a
 200-step Taylor-Green run on 3072 tets: reverse-sweep cost over the forward
 run, and a finite-difference check of the gradient).  `setup` compares the
 geometry builders on the workload mesh (GPU: wadg_geofacs + wadg_match_faces;
@@ -254,15 +254,16 @@ def run_ours(args):
         app.close()
         RP.finish(pg)
         return
-    # autotuner: the volume kernel's CTA shape, timed on this workload
-    vol_warps, vol_cand = app.autotune(dt)
-    app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     # warm-up (also captures the time-step graphs) and the choice between the
     # stage implementations: three reference kernels, the fused kernel, or
-    # the volume + surface kernel and the update kernel
-    variants = {}
+    # the volume + surface kernel and the update kernel; the first and the
+    # last with their volume kernel's CTA shape autotuned on this workload
+    variants, tuned = {}, {}
     for name in VARIANTS:
         app.set_stage_variant(name)
+        if name != "fused":
+            app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
+            tuned[name] = app.autotune(dt)
         app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
         app.rk_run(dt, max(args.warmup, 1), graph=True)
         variants[name] = app.time_run(dt, 10, graph=True) / 10
@@ -272,6 +273,9 @@ def run_ours(args):
     # every rank takes the same variant (rank 0's choice)
     pick = VARIANTS[int(RP.all_max(pg, VARIANTS.index(pick) if rank == 0 else 0))]
     app.set_stage_variant(pick)
+    if pick in tuned:
+        capi.check(capi.lib().wadg_ctx_set_vol_warps(capi.lib().wadg_app_ctx(app.h), 0, tuned[pick][0]),
+                   "set_vol_warps")
     app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     app.rk_run(dt, max(args.warmup, 1), graph=True)
     barrier()
@@ -374,8 +378,8 @@ def run_ours(args):
                             f"buffers, wall clock)",
                     "calls": e2e_calls},
             "gpu_launches": LAUNCHES[pick] * args.steps,
-            "autotune": {"vol_warps": vol_warps,
-                         "vol_ms_per_candidate": {str(w): t for w, t in vol_cand.items()}},
+            "autotune": {v: {"vol_warps": w, "ms_per_candidate": {str(k): t for k, t in c.items()}}
+                         for v, (w, c) in tuned.items()},
             "stage_variant": {"used": pick, "ms_per_step": variants},
             "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks, "setup": setup}
     if not args.no_ensemble:
@@ -470,50 +474,47 @@ def run_adjoint_measurement(nhex=8, nsteps=200, every=20, reps=3, fd_dirs=2):
                     "the checkpointed forward run"}
 
 
-def run_ensemble_measurement(steps=5, warmup=2):
+def run_ensemble_measurement(T=0.05, reps=2):
     """The batched-ensemble workload: 256 independent 2D vortex solves (K log-uniform in
-    [200, 8192], N uniform in {2,3,4}, seeded), batched (bins + one CUDA graph
-    per time step) against the plain one-instance-per-launch path, same dt and
-    steps; throughput in DOF*stages/s, timed with CUDA events."""
+    [200, 8192], N uniform in {2,3,4}, seeded), each run to the final time T with its
+    own step (the reference's dt per instance), batched (degree bins, work lists of
+    the instances still running, one CUDA graph per time step) against the plain
+    one-instance-per-launch path; throughput in DOF*stages/s over the whole run,
+    timed with CUDA events."""
     from scratch_wadge_b200 import ensemble as EN
     from scratch_wadge_b200 import geometry_gpu as GG
     t0 = time.perf_counter()
     inst = EN.draw_instances(n=256, kmin=200, kmax=8192, degrees=(2, 3, 4), seed=0)
     parts = [EN.build_instance(i, builder=GG.build_geometry_gpu) for i in inst]
-    dt = EN.common_dt(parts)
     setup_s = time.perf_counter() - t0
-    out = {"instances": len(inst), "K_total": sum(i.K for i in inst),
-           "degrees": {str(N): sum(1 for i in inst if i.N == N) for N in (2, 3, 4)},
-           "setup_s": setup_s, "steps": steps}
-    res, tuning = {}, {}
-    for fused in (False, True):
-        # three-kernel bins: the volume kernel's CTA shape autotuned per bin
-        ens = EN.Ensemble(inst, parts, fused=fused, autotune_dt=None if fused else dt)
-        if not fused:
-            tuning = {str(N): {"vol_warps": b["tuning"][0],
-                               "vol_ms_per_candidate": {str(w): t for w, t in b["tuning"][1].items()}}
-                      for N, b in ens.bins.items()}
-            if ens.joint_tuning:  # per-bin shapes against the defaults, bins run together
-                tuning["joint"] = ens.joint_tuning
-        ens.run(dt, warmup)
-        ms = ens.time_run(dt, steps)
-        res["fused" if fused else "three_kernels"] = ms / steps
-        dofs = ens.dofs
-        ens.close()
-    best = min(res.values())
-    single = EN.SingleInstances(inst, parts)
-    single.run(dt, 1)
-    ms_single = single.time_run(dt, max(2, steps // 2)) / max(2, steps // 2)
+    ens = EN.Ensemble(inst, parts, T=T, autotune=True)
+    nsteps = [n for _, n in ens.steps]
+    work = ens.stage_dofs
+    ens.run()  # warm-up (and the graph), then timed runs from the start
+    best = float("inf")
+    for _ in range(reps):
+        ens.restart()
+        best = min(best, ens.time_run())
+    ens_tuning = ens.tuning
+    ens.close()
+    single = EN.SingleInstances(inst, parts, T=T)
+    ms_single = single.time_run()
     single.close()
-    out.update({"dofs_per_field": dofs,
-                "batched_ms_per_step": best, "batched_variant_ms": res,
-                "batched_value": dofs * 5 / (best * 1e-3),
-                "single_ms_per_step": ms_single,
-                "single_value": dofs * 5 / (ms_single * 1e-3),
-                "speedup": ms_single / best, "unit": UNIT, "autotune": tuning,
-                "single_path": "one wadg_app per instance, 3 kernels x 5 stages launched per instance",
-                "batched_path": "one bin per degree (concatenated instances), one CUDA graph per step, bins on concurrent streams"})
-    return out
+    return {"instances": len(inst), "K_total": sum(i.K for i in inst),
+            "degrees": {str(N): sum(1 for i in inst if i.N == N) for N in (2, 3, 4)},
+            "final_time": T, "steps_per_instance": {"min": min(nsteps), "max": max(nsteps),
+                                                    "mean": sum(nsteps) / len(nsteps)},
+            "setup_s": setup_s, "dof_stages": work,
+            "batched_ms": best, "batched_value": work / (best * 1e-3),
+            "single_ms": ms_single, "single_value": work / (ms_single * 1e-3),
+            "speedup": ms_single / best, "unit": UNIT,
+            "autotune": {str(N): {"vol_warps": w, "ms_per_candidate": {str(k): t for k, t in c.items()}}
+                         for N, (w, c) in ens_tuning.items()},
+            "single_path": "one wadg_app per instance, 3 kernels x 5 stages launched per instance "
+                           "and step, each instance its own steps",
+            "batched_path": "one bin per degree (concatenated instances), volume + surface and "
+                            "update kernels over work lists of the batches still running, per-element "
+                            "steps, one CUDA graph per time step, bins on concurrent streams"}
 
 
 def fp64_peak(stream):

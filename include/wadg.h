@@ -433,12 +433,13 @@ int wadg_app_time_stage(wadg_app *app, double dt, int nstages, float *ms);
  * around every launch; ms[0..1] = total volume + surface, update time. */
 int wadg_app_time_volsurf(wadg_app *app, double dt, int nstages, float *ms);
 
-/* Autotuner: times `nstages` LSRK stages (three kernels, CUDA events) with
- * each compiled CTA shape of the volume kernel on the app's own mesh and
- * state, keeps the fastest (written to *warps; times, if not NULL, receives
- * the volume kernel's ms per launch for each candidate in the order of
- * wadg_vol_warps_candidates) and leaves it selected for the app's kernels.
- * Advances the app's state: call it before set_state. */
+/* Autotuner: times `nstages` LSRK stages (CUDA events) with each compiled
+ * CTA shape of the volume kernel -- or, in the volume + surface stage
+ * variant, of the volume + surface kernel, which has the same shapes -- on
+ * the app's own mesh and state, keeps the fastest (written to *warps; times,
+ * if not NULL, receives that kernel's ms per launch for each candidate in the
+ * order of wadg_vol_warps_candidates) and leaves it selected for the app's
+ * kernels.  Advances the app's state: call it before set_state. */
 int wadg_app_autotune(wadg_app *app, double dt, int nstages, int *warps,
                       float *times);
 
@@ -453,18 +454,39 @@ int wadg_app_set_parity(wadg_app *app, int parity);
 int wadg_app_get_fused(wadg_app *app);
 
 /* ------------------------------------------------------------ ensemble
- * Batched ensemble of independent solves.  A bin is one wadg_app holding the
- * concatenation of all instances of one degree (neighbour maps offset per
- * instance, one common dt); wadg_ensemble_run replays one CUDA graph per time
- * step whose branches -- one per bin, on the bins' own streams -- run
- * concurrently.  The reference runs one instance per process; no
- * counterpart. */
+ * Batched ensemble of independent solves, each instance with its own time
+ * step.  A bin is one wadg_app holding the concatenation of instances of one
+ * degree (neighbour maps offset per instance); instance i of a bin covers
+ * elements [offsets[i], offsets[i+1]) and makes nsteps[i] LSRK-45 steps of
+ * size dt[i] (per instance, e.g. the reference's dt = CFL hmin / C_N,
+ * euler.c:4180-4193, rounded to reach the final time).  Every bin runs the volume + surface
+ * kernel and the update kernel over work lists of the element batches that
+ * hold a running instance (an instance done is frozen: its step becomes 0 and
+ * the batches it alone occupied leave the lists); one CUDA graph per time step
+ * covers all bins, each on its app's stream, concurrently.  The apps must not
+ * use the fused stage variant.  The reference runs one instance per process;
+ * no counterpart.
+ *
+ * wadg_ensemble_run advances up to nsteps time steps (fewer once every
+ * instance is done); wadg_ensemble_steps reports the steps done and the
+ * longest instance's count; wadg_ensemble_restart sets the step count and
+ * the lists back to the start (the caller restores the apps' states). */
 typedef struct wadg_ensemble wadg_ensemble;
-int wadg_ensemble_create(int nbins, wadg_app **bins, wadg_ensemble **out);
+typedef struct
+{
+  wadg_app *app;
+  int ninst;
+  const int *offsets;  /* ninst + 1 element offsets, from 0 to the app's K */
+  const double *dt;    /* ninst steps, > 0 */
+  const int *nsteps;   /* ninst step counts, >= 0 */
+} wadg_ensemble_bin;
+int wadg_ensemble_create(int nbins, const wadg_ensemble_bin *bins, wadg_ensemble **out);
 int wadg_ensemble_destroy(wadg_ensemble *ens);
-int wadg_ensemble_run(wadg_ensemble *ens, double dt, int nsteps);
+int wadg_ensemble_run(wadg_ensemble *ens, int nsteps);
+int wadg_ensemble_restart(wadg_ensemble *ens);
+int wadg_ensemble_steps(const wadg_ensemble *ens, int *done, int *max_steps);
 int wadg_ensemble_sync(wadg_ensemble *ens);
-int wadg_ensemble_time_run(wadg_ensemble *ens, double dt, int nsteps, float *ms);
+int wadg_ensemble_time_run(wadg_ensemble *ens, int nsteps, float *ms);
 
 /* ------------------------------------------------------------ no allocation
  * One LSRK stage -- vol, surf and update, exactly what wadg_rk_step does --

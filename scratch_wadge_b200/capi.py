@@ -96,8 +96,13 @@ def lib():
         L.wadg_app_stream.argtypes = [v]
         L.wadg_app_set_parity.argtypes = [v, i]
         L.wadg_app_get_fused.argtypes = [v]
+        L.wadg_ensemble_create.argtypes = [i, v, ctypes.POINTER(ctypes.c_void_p)]
         L.wadg_ensemble_destroy.argtypes = [v]
         L.wadg_ensemble_sync.argtypes = [v]
+        L.wadg_ensemble_run.argtypes = [v, i]
+        L.wadg_ensemble_restart.argtypes = [v]
+        L.wadg_ensemble_steps.argtypes = [v, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.wadg_ensemble_time_run.argtypes = [v, i, ctypes.POINTER(ctypes.c_float)]
         L.wadg_app_create.argtypes = [ctypes.POINTER(Params), i, i, ctypes.POINTER(HostData),
                                       ctypes.POINTER(ctypes.c_void_p)]
         L.wadg_ctx_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(ctypes.c_void_p)]

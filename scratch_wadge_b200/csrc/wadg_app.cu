@@ -493,11 +493,14 @@ int wadg_app_autotune(wadg_app *a, double dt, int nstages, int *warps, float *ti
   if (n <= 0) return afail(WADG_ERR_UNSUPPORTED, "no volume kernel shapes");
   int best = cand[0];
   float best_ms = -1.0f;
+  // the volume kernel's time, or (volume + surface variant) the volume +
+  // surface kernel's
+  const bool vs = a->fused == WADG_STAGE_VOLSURF;
   for (int i = 0; i < n; ++i) {
     int r = wadg_ctx_set_vol_warps(a->ctx, a->curved, cand[i]);
     float ms[3] = {0, 0, 0};
-    if (!r) r = wadg_app_time_kernels(a, dt, 1, ms);  // warm-up: attributes, caches
-    if (!r) r = wadg_app_time_kernels(a, dt, nstages, ms);
+    if (!r) r = vs ? wadg_app_time_volsurf(a, dt, 1, ms) : wadg_app_time_kernels(a, dt, 1, ms);
+    if (!r) r = vs ? wadg_app_time_volsurf(a, dt, nstages, ms) : wadg_app_time_kernels(a, dt, nstages, ms);
     if (r) return r;
     if (times) times[i] = ms[0] / nstages;
     if (best_ms < 0.0f || ms[0] < best_ms) {

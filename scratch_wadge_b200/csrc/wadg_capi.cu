@@ -93,7 +93,8 @@ int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const doubl
                        const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
                        const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
                        const double *Qf, double *rhsQ, double *rhsQf,
-                       const double *fgeo = nullptr, const uint32_t *mapPq = nullptr) {
+                       const double *fgeo = nullptr, const uint32_t *mapPq = nullptr,
+                       const int *blist = nullptr, const int *nb = nullptr) {
   using C = VolPairsCfg<DIM, N, CURVED, W>;
   static_assert(C::smem_vol <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
   auto kern = vol_pairs_kernel<DIM, N, CURVED, W, SURF>;
@@ -106,19 +107,29 @@ int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const doubl
   const int grid = persistent_grid(K, C::E, C::smem_vol);
   kern<<<grid, C::threads, C::smem_vol, c->stream>>>(K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq,
                                                       VqLq, VfPq, Qf, rhsQ, rhsQf, c->phys, fgeo,
-                                                      mapPq);
+                                                      mapPq, blist, nb);
   return after_launch(SURF ? "volume + surface kernel" : "volume kernel");
 }
 
-// the volume + surface kernel, in the default CTA shape
+// the volume + surface kernel in the context's CTA shape (wadg_ctx_set_vol_warps)
 template <int DIM, int N, bool CURVED>
 int launch_volsurf(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
                    const double *fgeo, const uint32_t *mapPq, const double *nrJ,
                    const double *nsJ, const double *ntJ, const double *Drq, const double *Dsq,
                    const double *Dtq, const double *VqLq, const double *VfPq, const double *Qf,
-                   double *rhsQ) {
+                   double *rhsQ, const int *blist = nullptr, const int *nb = nullptr) {
+  constexpr int W1 = volpairsW_cand<DIM, N, CURVED>(1), W2 = volpairsW_cand<DIM, N, CURVED>(2);
+  if (W1 && c->vol_warps == W1)
+    return launch_vol_pairs_w<DIM, N, CURVED, (W1 ? W1 : 2), true>(
+        c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo, mapPq,
+        blist, nb);
+  if (W2 && c->vol_warps == W2)
+    return launch_vol_pairs_w<DIM, N, CURVED, (W2 ? W2 : 2), true>(
+        c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo, mapPq,
+        blist, nb);
   return launch_vol_pairs_w<DIM, N, CURVED, volpairsW<DIM, N, CURVED>(), true>(
-      c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo, mapPq);
+      c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo, mapPq,
+      blist, nb);
 }
 
 // the context's CTA shape (wadg_ctx_set_vol_warps), else the default
@@ -223,8 +234,10 @@ int kernel_shape(const wadg_ctx *c, int kernel, int K, int *E, int *grid) {
     case WADG_KERNEL_UPDATE:
       *E = UpdMmaCfg<DIM, N, CURVED>::EW;
       return update_grid<DIM, N, CURVED>(K, grid);
-    case WADG_KERNEL_VOLSURF:
-      vol_shape<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>(K, E, grid);
+    case WADG_KERNEL_VOLSURF:  // the same CTA shapes as the volume kernel
+      if (W1 && c->vol_warps == W1) vol_shape<DIM, N, CURVED, (W1 ? W1 : 2)>(K, E, grid);
+      else if (W2 && c->vol_warps == W2) vol_shape<DIM, N, CURVED, (W2 ? W2 : 2)>(K, E, grid);
+      else vol_shape<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>(K, E, grid);
       return WADG_OK;
     case WADG_KERNEL_ADJ_PAIRS:
       return wadg_internal::adj_pairs_shape(DIM, N, CURVED, K, E, grid);
@@ -241,14 +254,15 @@ int kernel_shape(const wadg_ctx *c, int kernel, int K, int *E, int *grid) {
 template <int DIM, int N, bool CURVED>
 int launch_update(const wadg_ctx *c, int K, const double *Jq, const double *VqPq,
                   const double *VfPq, double fa, double fb, double fdt, double *rhsQ,
-                  double *resQ, double *Q, double *Qf) {
+                  double *resQ, double *Q, double *Qf, const double *dtK = nullptr,
+                  const int *glist = nullptr, const int *ng = nullptr) {
   using C = UpdMmaCfg<DIM, N, CURVED>;
   static_assert(C::smem <= 227 * 1024, "update kernel does not fit in shared memory");
   auto kern = update_mma_kernel<DIM, N, CURVED>;
   int grid = 0;
   if (int r = update_grid<DIM, N, CURVED>(K, &grid)) return r;
   kern<<<grid, C::threads, C::smem, c->stream>>>(K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q,
-                                                 Qf, c->phys);
+                                                 Qf, c->phys, dtK, glist, ng);
   return after_launch("update kernel");
 }
 
@@ -307,6 +321,40 @@ int wadg_ctx_sizes(const wadg_ctx *c, int *dim, int *NfqNf) {
 
 // the stream a context's kernels run on (used by wadg_noalloc.cu)
 cudaStream_t wadg_ctx_stream(const wadg_ctx *c) { return c ? c->stream : nullptr; }
+
+namespace wadg_internal {
+// The ensemble's stage kernels over work lists (wadg_ensemble.cu): the volume
+// + surface kernel over the volume batches blist[0 .. *nb) (ascending batch
+// indices of elems_per_batch(WADG_KERNEL_VOLSURF) elements), then the update
+// over the groups glist[0 .. *ng) with the step of element k in dtK[k].
+int volsurf_list(const wadg_ctx *c, int K, int curved, const double *vgeo, const double *vfgeo,
+                 const double *fgeo, const uint32_t *mapPq, const double *nrJ, const double *nsJ,
+                 const double *ntJ, const double *Drq, const double *Dsq, const double *Dtq,
+                 const double *VqLq, const double *VfPq, const double *Qf, double *rhsQ,
+                 const int *blist, const int *nb) {
+  if (int r = check_ctx(c, c ? c->dim : 0, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (curved)
+    WADG_DISPATCH(c, return (launch_volsurf<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ,
+                                                           Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, blist,
+                                                           nb)));
+  WADG_DISPATCH(c, return (launch_volsurf<D_, N_, false>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ,
+                                                          Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, blist,
+                                                          nb)));
+}
+
+int update_list(const wadg_ctx *c, int K, int curved, const double *Jq, const double *VqPq,
+                const double *VfPq, double fa, double fb, const double *dtK, double *rhsQ,
+                double *resQ, double *Q, double *Qf, const int *glist, const int *ng) {
+  if (int r = check_ctx(c, c ? c->dim : 0, K)) return r;
+  if (K == 0) return WADG_OK;
+  if (curved)
+    WADG_DISPATCH(c, return (launch_update<D_, N_, true>(c, K, Jq, VqPq, VfPq, fa, fb, 0.0, rhsQ, resQ,
+                                                          Q, Qf, dtK, glist, ng)));
+  WADG_DISPATCH(c, return (launch_update<D_, N_, false>(c, K, Jq, VqPq, VfPq, fa, fb, 0.0, rhsQ, resQ,
+                                                         Q, Qf, dtK, glist, ng)));
+}
+}  // namespace wadg_internal
 
 // per-element integrals (wadg_euler_3d_compute_aux, wadg_element_entropy)
 template <int DIM, int N, bool ENTROPY>

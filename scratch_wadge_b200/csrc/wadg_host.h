@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 namespace wadg_internal {
 
@@ -44,6 +45,20 @@ inline int sm_count() {
   }
   return c;
 }
+
+}  // namespace wadg_internal
+
+struct wadg_ctx;
+namespace wadg_internal {
+// the ensemble's stage kernels over work lists (wadg_capi.cu)
+int volsurf_list(const wadg_ctx *c, int K, int curved, const double *vgeo, const double *vfgeo,
+                 const double *fgeo, const uint32_t *mapPq, const double *nrJ, const double *nsJ,
+                 const double *ntJ, const double *Drq, const double *Dsq, const double *Dtq,
+                 const double *VqLq, const double *VfPq, const double *Qf, double *rhsQ,
+                 const int *blist, const int *nb);
+int update_list(const wadg_ctx *c, int K, int curved, const double *Jq, const double *VqPq,
+                const double *VfPq, double fa, double fb, const double *dtK, double *rhsQ,
+                double *resQ, double *Q, double *Qf, const int *glist, const int *ng);
 
 // launch shape (elements per batch, CTAs) of the adjoint's pair VJP kernel
 // for K elements (wadg_adjoint.cu)

@@ -171,13 +171,17 @@ __device__ __forceinline__ void update_group(
     const double *__restrict__ VqPq, const double *__restrict__ VfPq, double fa, double fb,
     double fdt, double *__restrict__ resQ, double *__restrict__ Q, double *__restrict__ rhsQ_out,
     double *__restrict__ Qf_out, const Phys &P, double (*res0)[DIM + 2], double (*q0)[DIM + 2],
-    double *Jv) {
+    double *Jv, const double *__restrict__ dtK = nullptr) {
   using C = UpdMmaCfg<DIM, N, CURVED>;
   constexpr int Nq = C::Nq, NF = C::NF, Nf = C::Nf, EW = C::EW, KS = C::KS, LD = C::LD,
                 MQ = C::MQ, MO = C::MO, W = C::WARPS;
   bool ev[2];
+  double dte[2];  // the step of the lane's two elements: fdt, or per element (dtK)
 #pragma unroll
-  for (int i = 0; i < 2; ++i) ev[i] = 2 * (lane & 3) + i < ne;
+  for (int i = 0; i < 2; ++i) {
+    ev[i] = 2 * (lane & 3) + i < ne;
+    dte[i] = (dtK && ev[i]) ? dtK[k0 + 2 * (lane & 3) + i] : fdt;
+  }
 
   double a[KS], D[Nf][2];
   // ---- r = M^{-1} rhs (affine: -2 VqPq rhs / J; WADG: VqPq(-2 VqPq rhs / J))
@@ -209,7 +213,7 @@ __device__ __forceinline__ void update_group(
 #pragma unroll
         for (int f = 0; f < Nf; ++f) {
           const double r = CURVED ? D[f][i] : m2J * D[f][i];
-          const double res = fa * res0[i][f] + fdt * r;
+          const double res = fa * res0[i][f] + dte[i] * r;
           U[f] = q0[i][f] + fb * res;
           if (ev[i]) {
             resQ[id + f * Nq] = res;
@@ -302,7 +306,8 @@ __global__ void __launch_bounds__(UpdMmaCfg<DIM, N, CURVED>::threads, UpdMmaCfg<
 update_mma_kernel(int K, const double *__restrict__ Jq, const double *__restrict__ VqPq,
                   const double *__restrict__ VfPq, double fa, double fb, double fdt,
                   double *__restrict__ rhsQ, double *__restrict__ resQ, double *__restrict__ Q,
-                  double *__restrict__ Qf, Phys P) {
+                  double *__restrict__ Qf, Phys P, const double *__restrict__ dtK = nullptr,
+                  const int *__restrict__ blist = nullptr, const int *__restrict__ nblist = nullptr) {
   using C = UpdMmaCfg<DIM, N, CURVED>;
   constexpr int Nq = C::Nq, Nf = C::Nf, EW = C::EW, KP = C::KP, LD = C::LD, MQ = C::MQ;
   extern __shared__ double smem[];
@@ -315,9 +320,11 @@ update_mma_kernel(int K, const double *__restrict__ Jq, const double *__restrict
     Y[Nq * LD + t] = 0.0;
   }
 
-  const int ngroups = (K + EW - 1) / EW;
-  for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
-    const int k0 = g * EW;
+  // the groups to run: all of them, or (a work list: the ensemble's active
+  // instances) the group indices blist[0 .. *nblist); dtK: a step per element
+  const int ngroups = blist ? *nblist : (K + EW - 1) / EW;
+  for (int ig = blockIdx.x; ig < ngroups; ig += gridDim.x) {
+    const int k0 = (blist ? blist[ig] : ig) * EW;
     const int ne = min(EW, K - k0);
     // the LSRK operands of this warp's first m-tile load alongside the rhs block
     double res0[2][Nf], q0[2][Nf], Jv[2];
@@ -326,7 +333,7 @@ update_mma_kernel(int K, const double *__restrict__ Jq, const double *__restrict
     });
     __syncthreads();
     update_group<DIM, N, CURVED>(k0, ne, warp, lane, X, Y, Jq, VqPq, VfPq, fa, fb, fdt, resQ, Q,
-                                 rhsQ, Qf, P, res0, q0, Jv);
+                                 rhsQ, Qf, P, res0, q0, Jv, dtK);
   }
 }
 

@@ -422,7 +422,8 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
                  const double *__restrict__ VqLq, const double *__restrict__ VfPq,
                  const double *__restrict__ Qf, double *__restrict__ rhsQ,
                  double *__restrict__ rhsQf, Phys P, const double *__restrict__ fgeo = nullptr,
-                 const uint32_t *__restrict__ mapPq = nullptr) {
+                 const uint32_t *__restrict__ mapPq = nullptr,
+                 const int *__restrict__ blist = nullptr, const int *__restrict__ nblist = nullptr) {
   using V = VolPairs<DIM, N, CURVED, W>;
   constexpr int Nq = V::Nq, NF = V::NF, Nf = V::Nf, R = V::R, L = V::L, E = V::E, H = V::H;
   extern __shared__ double smem[];
@@ -454,9 +455,14 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     cp_async_commit();
   };
   __syncthreads();  // the tables are shared by every group
-  if (PRE) prefetch_group(blockIdx.x * E);
+  // the batches to run: all of them, or (a work list: the ensemble's active
+  // instances) the ascending batch indices blist[0 .. *nblist)
+  const int nb = blist ? *nblist : (K + E - 1) / E;
+  auto batch = [&](int i) { return i < nb ? (blist ? blist[i] : i) * E : K; };
+  if (PRE) prefetch_group(batch(blockIdx.x));
 
-  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
+  for (int ib = blockIdx.x; ib < nb; ib += gridDim.x) {
+    const int k0 = batch(ib);
     if (PRE) cp_async_wait_all();
     // a group whose elements all lie past the end (the CTA's last batch) has
     // nothing to compute, and must not read element K-1's input, which the
@@ -465,7 +471,7 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     gsync();  // the group's traces staged / its previous batch done with its shared memory
     v.prologue_range(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P, PRE ? v.sPre : nullptr);
     gsync();
-    if (PRE) prefetch_group(k0 + gridDim.x * E);  // the next batch's traces, during the pairs
+    if (PRE) prefetch_group(batch(ib + gridDim.x));  // the next batch's traces, during the pairs
     double acc[R][Nf];
     v.pairs(acc, P);
     gsync();  // the group's pairs done: its state block becomes the row buffer

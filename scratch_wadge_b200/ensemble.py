@@ -6,14 +6,17 @@ vortex strength and centre.  Instances of one degree form a *bin*: their
 geometry and state arrays are concatenated and their neighbour maps offset,
 so the bin is one element list that the persistent kernels walk without
 knowing instance boundaries (every kernel is element-local apart from the
-mapPq gather, which stays inside its instance).  All instances advance with
-one common dt (the smallest stable one), so a bin is exactly one solver.
+mapPq gather, which stays inside its instance).  Every instance runs to the
+common final time T with its own step (the reference's dt with the
+instance's wave speed); the
+kernels take the step per element and walk work lists of the batches of
+instances still running.
 
 ``Ensemble``          the batched path: one wadg_app per bin, one CUDA graph
                       per time step covering all bins (wadg_ensemble_run).
 ``SingleInstances``   the plain path: one wadg_app per instance, each time
                       step launched instance by instance (3 kernels x 5
-                      stages x instances).
+                      stages x instances), each instance its own steps.
 """
 
 from __future__ import annotations
@@ -84,87 +87,66 @@ def concat(parts):
     return geo, st, offs
 
 
-def common_dt(parts, CFL=0.5):
-    """Smallest stable step over the instances (wave-speed scaled)."""
-    dts = []
-    for geo, st in parts:
-        dt, _ = IC.time_step(geo, CFL, geo.ops.N, nsteps=1, wave_speed=IC.max_wave_speed(st["Q"]))
-        dts.append(dt)
-    return min(dts)
+def instance_steps(parts, T, CFL=0.5):
+    """Each instance's own step and step count to the final time T: the
+    reference's dt = CFL hmin / C_N (euler.c:4180-4193) divided by the
+    instance's largest wave speed |u| + c, then n = ceil(T / dt) and
+    dt = T / n (euler.c:3680-3688).  Without the wave speed the coarsest
+    instances (a few dozen triangles, |u| + c up to 2.5) blow up within one
+    step."""
+    return [IC.time_step(geo, CFL, geo.ops.N, FinalTime=T, wave_speed=IC.max_wave_speed(st["Q"]))
+            for geo, st in parts]
 
 
 class Ensemble:
-    """The batched path."""
+    """The batched path: one wadg_app per degree bin, every instance with its
+    own step to the final time T (wadg_ensemble_*)."""
 
-    def __init__(self, instances, parts=None, fused=False, gamma=1.4, autotune_dt=None):
+    def __init__(self, instances, parts=None, T=0.1, CFL=0.5, gamma=1.4, autotune=False):
+        """autotune: pick each bin's CTA shape of the volume + surface kernel
+        by timing it on the bin (wadg_app_autotune)"""
         self.instances = instances
         self.parts = parts if parts is not None else [build_instance(i, gamma) for i in instances]
+        self.steps = instance_steps(self.parts, T, CFL)
+        self.T = T
         self.degrees = sorted({i.N for i in instances})
         self.bins = {}
+        self.tuning = {}
         for N in self.degrees:
             idx = [j for j, i in enumerate(instances) if i.N == N]
             geo, st, offs = concat([self.parts[j] for j in idx])
             app = capi.App(geo, curved=True, gamma=gamma)
-            app.set_fused(fused)
-            tuning = None
-            if autotune_dt is not None:  # the volume kernel's CTA shape for this bin
+            app.set_stage_variant("volsurf")
+            if autotune:
                 app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
-                tuning = app.autotune(autotune_dt)
+                self.tuning[N] = app.autotune(min(self.steps[j][0] for j in idx))
             app.set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
-            self.bins[N] = dict(idx=idx, geo=geo, state=st, offs=offs, app=app, tuning=tuning)
-        self.h = None
-        self.joint_tuning = None
-        if autotune_dt is not None:
-            self._tune_jointly(autotune_dt)
+            self.bins[N] = dict(idx=idx, geo=geo, state=st, offs=offs, app=app,
+                                dt=np.array([self.steps[j][0] for j in idx], dtype=np.float64),
+                                nsteps=np.array([self.steps[j][1] for j in idx], dtype=np.int32),
+                                offs32=np.ascontiguousarray(offs, dtype=np.int32))
         self.h = self._create()
         self.K = sum(g.K for g, _ in self.parts)
         self.dofs = sum(g.K * g.ops.Np for g, _ in self.parts)
 
+    @property
+    def stage_dofs(self):
+        """DOF x stages of the whole run to T (each instance its own steps)."""
+        return sum(g.K * g.ops.Np * 5 * n for (g, _), (_, n) in zip(self.parts, self.steps))
+
     def _create(self):
-        apps = (ctypes.c_void_p * len(self.bins))(*[b["app"].h.value for b in self.bins.values()])
+        L = capi.lib()
+        descs = (EnsembleBin * len(self.bins))()
+        for d, b in zip(descs, self.bins.values()):
+            d.app = b["app"].h.value
+            d.ninst = len(b["idx"])
+            d.offsets = b["offs32"].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+            d.dt = b["dt"].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            d.nsteps = b["nsteps"].ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         h = ctypes.c_void_p()
-        L = capi.lib()
-        L.wadg_ensemble_create.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
-        capi.check(L.wadg_ensemble_create(len(self.bins), apps, ctypes.byref(h)), "ensemble_create")
+        capi.check(L.wadg_ensemble_create(len(self.bins), ctypes.cast(descs, ctypes.c_void_p),
+                                          ctypes.byref(h)), "ensemble_create")
         return h
-
-    def _set_shapes(self, shapes):
-        L = capi.lib()
-        for N, b in self.bins.items():
-            ctx = ctypes.c_void_p(L.wadg_app_ctx(b["app"].h))
-            capi.check(L.wadg_ctx_set_vol_warps(ctx, 1, shapes[N]), "set_vol_warps")
-
-    def _tune_jointly(self, dt, steps=3):
-        """Each bin's shape was tuned alone, but the bins run concurrently:
-        keep the per-bin choices only if the whole batched step is faster
-        with them than with every bin at its default shape."""
-        tuned = {N: b["tuning"][0] for N, b in self.bins.items()}
-        default = {N: 0 for N in self.bins}
-        if all(tuned[N] == self._default_shape(N) for N in self.bins):
-            return
-        times = {}
-        L = capi.lib()
-        for name, shapes in (("tuned", tuned), ("default", default)):
-            self._set_shapes(shapes)
-            h = self._create()
-            self.h = h
-            try:
-                self.run(dt, 1)
-                times[name] = self.time_run(dt, steps) / steps
-            finally:
-                L.wadg_ensemble_destroy(h)
-                self.h = None
-        best = "tuned" if times["tuned"] <= times["default"] else "default"
-        self._set_shapes(tuned if best == "tuned" else default)
-        self.joint_tuning = dict(ms_per_step=times, kept=best)
-        self.reset()
-
-    def _default_shape(self, N):
-        L = capi.lib()
-        ctx = ctypes.c_void_p(L.wadg_app_ctx(self.bins[N]["app"].h))
-        cand = (ctypes.c_int * 3)()
-        L.wadg_vol_warps_candidates(ctx, 1, cand)
-        return int(cand[0])
 
     def close(self):
         if getattr(self, "h", None):
@@ -175,23 +157,32 @@ class Ensemble:
 
     __del__ = close
 
-    def reset(self):
+    def restart(self):
+        """Back to the initial states and step 0."""
         for b in self.bins.values():
             st = b["state"]
             b["app"].set_state(st["Q"], st["rhsQ"], st["Qf"], st["resQ"])
+        capi.check(capi.lib().wadg_ensemble_restart(self.h), "ensemble_restart")
 
-    def run(self, dt, nsteps):
+    def progress(self):
+        """(time steps done, the longest instance's step count)"""
+        done, mx = ctypes.c_int(), ctypes.c_int()
+        capi.check(capi.lib().wadg_ensemble_steps(self.h, ctypes.byref(done), ctypes.byref(mx)),
+                   "ensemble_steps")
+        return done.value, mx.value
+
+    def run(self, nsteps=None):
+        """Advance nsteps time steps (None: to the end of every instance)."""
         L = capi.lib()
-        L.wadg_ensemble_run.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
-        capi.check(L.wadg_ensemble_run(self.h, dt, nsteps), "ensemble_run")
+        n = self.progress()[1] if nsteps is None else nsteps
+        capi.check(L.wadg_ensemble_run(self.h, n), "ensemble_run")
         capi.check(L.wadg_ensemble_sync(self.h), "ensemble_sync")
 
-    def time_run(self, dt, nsteps):
-        L = capi.lib()
-        L.wadg_ensemble_time_run.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
-                                             ctypes.POINTER(ctypes.c_float)]
+    def time_run(self, nsteps=None):
+        """Device time (ms) of nsteps time steps (None: to the end)."""
         ms = ctypes.c_float()
-        capi.check(L.wadg_ensemble_time_run(self.h, dt, nsteps, ctypes.byref(ms)), "ensemble_time_run")
+        n = self.progress()[1] if nsteps is None else nsteps
+        capi.check(capi.lib().wadg_ensemble_time_run(self.h, n, ctypes.byref(ms)), "ensemble_time_run")
         return ms.value
 
     def instance_state(self, j):
@@ -204,13 +195,22 @@ class Ensemble:
         return {k: v[a:z] for k, v in s.items()}
 
 
-class SingleInstances:
-    """The plain path: one solver per instance, launched one after another."""
+class EnsembleBin(ctypes.Structure):
+    _fields_ = [("app", ctypes.c_void_p), ("ninst", ctypes.c_int),
+                ("offsets", ctypes.POINTER(ctypes.c_int)), ("dt", ctypes.POINTER(ctypes.c_double)),
+                ("nsteps", ctypes.POINTER(ctypes.c_int))]
 
-    def __init__(self, instances, parts=None, gamma=1.4):
+
+class SingleInstances:
+    """The plain path: one solver per instance, launched one after another,
+    each with its own step to the final time T."""
+
+    def __init__(self, instances, parts=None, T=0.1, CFL=0.5, gamma=1.4):
         import torch
         self.instances = instances
         self.parts = parts if parts is not None else [build_instance(i, gamma) for i in instances]
+        self.steps = instance_steps(self.parts, T, CFL)
+        self.done = [0] * len(self.parts)
         self.stream = torch.cuda.Stream()  # one stream for all instances, in order
         self.apps = []
         for geo, st in self.parts:
@@ -225,21 +225,27 @@ class SingleInstances:
         for a in self.apps:
             a.close()
 
-    def run(self, dt, nsteps):
-        for _ in range(nsteps):
-            for a in self.apps:
-                a.rk_run(dt, 1, graph=False)
+    def _advance(self, nsteps):
+        for j, a in enumerate(self.apps):
+            dt, n = self.steps[j]
+            m = n - self.done[j] if nsteps is None else min(nsteps, n - self.done[j])
+            if m > 0:
+                a.rk_run(dt, m, graph=False)
+                self.done[j] += m
+
+    def run(self, nsteps=None):
+        """Advance every instance by nsteps of its own steps, at most to its
+        end (None: to the end)."""
+        self._advance(nsteps)
         self.apps[0].sync()
 
-    def time_run(self, dt, nsteps):
-        """Device time of nsteps on the shared stream (CUDA events)."""
+    def time_run(self):
+        """Device time (ms) of the whole run to T on the shared stream."""
         import torch
         s = self.stream
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        for _ in range(nsteps):
-            for a in self.apps:
-                a.rk_run(dt, 1, graph=False)
+        self._advance(None)
         e1.record(s)
         e1.synchronize()
         return e0.elapsed_time(e1)
