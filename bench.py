@@ -248,7 +248,11 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     if args.profile:
-        # a short run for profilers: warm-up and a few time steps, nothing else
+        # a short run for profilers: warm-up and a few time steps (in the
+        # stage variant --stage-variant names; three kernels for auto),
+        # nothing else
+        if args.stage_variant != "auto":
+            app.set_stage_variant(args.stage_variant)
         app.rk_run(dt, args.warmup + args.steps, graph=False)
         barrier()
         app.close()
