@@ -267,7 +267,8 @@ def run_ours(args):
         app.set_stage_variant(name)
         if name != "fused":
             app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
-            tuned[name] = app.autotune(dt)
+            label, times = app.autotune(dt)
+            tuned[name] = (label, times, app.vol_shape())
         app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
         app.rk_run(dt, max(args.warmup, 1), graph=True)
         variants[name] = app.time_run(dt, 10, graph=True) / 10
@@ -278,8 +279,7 @@ def run_ours(args):
     pick = VARIANTS[int(RP.all_max(pg, VARIANTS.index(pick) if rank == 0 else 0))]
     app.set_stage_variant(pick)
     if pick in tuned:
-        capi.check(capi.lib().wadg_ctx_set_vol_warps(capi.lib().wadg_app_ctx(app.h), 0, tuned[pick][0]),
-                   "set_vol_warps")
+        app.set_vol_shape(*tuned[pick][2])
     app.set_state(st0["Q"], st0["rhsQ"], st0["Qf"], st0["resQ"])
     app.rk_run(dt, max(args.warmup, 1), graph=True)
     barrier()
@@ -382,14 +382,16 @@ def run_ours(args):
                             f"buffers, wall clock)",
                     "calls": e2e_calls},
             "gpu_launches": LAUNCHES[pick] * args.steps,
-            "autotune": {v: {"vol_warps": w, "ms_per_candidate": {str(k): t for k, t in c.items()}}
-                         for v, (w, c) in tuned.items()},
+            "autotune": {v: {"vol_shape": w, "ms_per_shape": c} for v, (w, c, _) in tuned.items()},
             "stage_variant": {"used": pick, "ms_per_step": variants},
             "roofline": roof, "hbm_kernels": hbm_kernels, "clocks": clocks, "setup": setup}
     if not args.no_ensemble:
         line["ensemble"] = run_ensemble_measurement()
     if not args.no_adjoint:
         line["adjoint"] = run_adjoint_measurement()
+        # the bench workload's own size: 40 steps, checkpoint every 20
+        line["adjoint_K24576"] = run_adjoint_measurement(nhex=NHEX, nsteps=40, every=20, reps=2,
+                                                         fd_dirs=1)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(cpu_threads()))
         sec, kind = time_cpu(geo, st0, dt, 2)
@@ -405,8 +407,9 @@ def run_ours(args):
 
 def run_adjoint_measurement(nhex=8, nsteps=200, every=20, reps=3, fd_dirs=2):
     """Discrete adjoint of the Taylor-Green run: gradient of J = int rho(T)^2
-    with respect to the initial state on 8^3 x 6 = 3072 affine tets, N = 3,
-    200 LSRK-45 steps, checkpoint every 20 steps.  Times (CUDA events on the
+    with respect to the initial state on nhex^3 x 6 affine tets (3072 by
+    default), N = 3, nsteps LSRK-45 steps (200), checkpoint every `every`
+    steps (20); the time steps run the volume + surface stage variant.  Times (CUDA events on the
     app's stream, best of `reps`): the plain forward run (graph-replayed), the
     checkpointed forward run and the reverse sweep (segment recompute + stage
     adjoints).  `fd_check`: relative difference of dJ/dQ0 . d from central
@@ -423,6 +426,7 @@ def run_adjoint_measurement(nhex=8, nsteps=200, every=20, reps=3, fd_dirs=2):
     Q0 = IC.stage0(geo, IC.initial_state(geo, "taylor_green"))[0]
     dt = IC.time_step(geo, CFL, N, nsteps=nsteps, wave_speed=IC.max_wave_speed(Q0))[0]
     app = capi.App(geo, False)
+    app.set_stage_variant("volsurf")  # the forward run and the recompute alike
     adj = Adjoint(app, nsteps, every)
     Qd = torch.from_numpy(Q0).cuda()
     stream = torch.cuda.ExternalStream(capi.lib().wadg_app_stream(app.h))
@@ -512,8 +516,7 @@ def run_ensemble_measurement(T=0.05, reps=2):
             "batched_ms": best, "batched_value": work / (best * 1e-3),
             "single_ms": ms_single, "single_value": work / (ms_single * 1e-3),
             "speedup": ms_single / best, "unit": UNIT,
-            "autotune": {str(N): {"vol_warps": w, "ms_per_candidate": {str(k): t for k, t in c.items()}}
-                         for N, (w, c) in ens_tuning.items()},
+            "autotune": {str(N): {"vol_shape": w, "ms_per_shape": c} for N, (w, c) in ens_tuning.items()},
             "single_path": "one wadg_app per instance, 3 kernels x 5 stages launched per instance "
                            "and step, each instance its own steps",
             "batched_path": "one bin per degree (concatenated instances), volume + surface and "

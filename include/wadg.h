@@ -68,6 +68,17 @@ int wadg_ctx_set_stream(wadg_ctx *ctx, void *stream);
 int wadg_vol_warps_candidates(const wadg_ctx *ctx, int curved, int *out);
 int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps);
 int wadg_ctx_get_vol_warps(const wadg_ctx *ctx);
+/* Its node-to-thread map is a second axis: L lanes per element with R rows
+ * each (by default about three rows per lane).  wadg_vol_shapes writes every
+ * compiled (warps, rows) pair -- first those of wadg_vol_warps_candidates with
+ * rows 0 (the default map), then the other maps where they fill the lanes
+ * with less padding (2D N=4: 2 and 4 rows per lane for its 16 nodes) -- and
+ * returns their number (at most WADG_MAX_VOL_SHAPES);
+ * wadg_ctx_set_vol_shape selects one (rows 0: as wadg_ctx_set_vol_warps). */
+#define WADG_MAX_VOL_SHAPES 5
+int wadg_vol_shapes(const wadg_ctx *ctx, int curved, int *warps, int *rows);
+int wadg_ctx_set_vol_shape(wadg_ctx *ctx, int curved, int warps, int rows);
+int wadg_ctx_get_vol_rows(const wadg_ctx *ctx);
 /* Launch shape of one kernel for K elements, the numbers its entry point
  * uses: elements per batch (one CTA pass) and CTAs launched.  The volume,
  * update and fused stage kernels are persistent: CTA b takes batches b,
@@ -436,10 +447,12 @@ int wadg_app_time_volsurf(wadg_app *app, double dt, int nstages, float *ms);
 /* Autotuner: times `nstages` LSRK stages (CUDA events) with each compiled
  * CTA shape of the volume kernel -- or, in the volume + surface stage
  * variant, of the volume + surface kernel, which has the same shapes -- on
- * the app's own mesh and state, keeps the fastest (written to *warps; times,
- * if not NULL, receives that kernel's ms per launch for each candidate in the
- * order of wadg_vol_warps_candidates) and leaves it selected for the app's
- * kernels.  Advances the app's state: call it before set_state. */
+ * the app's own mesh and state, over every shape of wadg_vol_shapes (CTA
+ * size and node-to-thread map), keeps the fastest (its warps written to
+ * *warps, its rows to be read with wadg_ctx_get_vol_rows; times, if not NULL,
+ * an array of WADG_MAX_VOL_SHAPES, receives that kernel's ms per launch for
+ * each shape in the order of wadg_vol_shapes) and leaves it selected for the
+ * app's kernels.  Advances the app's state: call it before set_state. */
 int wadg_app_autotune(wadg_app *app, double dt, int nstages, int *warps,
                       float *times);
 

@@ -117,6 +117,9 @@ def lib():
         L.wadg_vol_warps_candidates.argtypes = [v, i, ctypes.POINTER(ctypes.c_int)]
         L.wadg_ctx_set_vol_warps.argtypes = [v, i, i]
         L.wadg_ctx_get_vol_warps.argtypes = [v]
+        L.wadg_vol_shapes.argtypes = [v, i, ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.wadg_ctx_set_vol_shape.argtypes = [v, i, i, i]
+        L.wadg_ctx_get_vol_rows.argtypes = [v]
         L.wadg_check_state.argtypes = [v, i, v, v, ctypes.POINTER(i), ctypes.POINTER(i)]
         L.wadg_app_check_state.argtypes = [v, ctypes.POINTER(i), ctypes.POINTER(i)]
         L.wadg_app_set_check_every.argtypes = [v, i]
@@ -256,6 +259,12 @@ class Context:
     def set_vol_warps(self, curved, warps):
         check(lib().wadg_ctx_set_vol_warps(self.h, int(curved), warps), "set_vol_warps")
 
+    def set_vol_shape(self, curved, warps, rows):
+        check(lib().wadg_ctx_set_vol_shape(self.h, int(curved), warps, rows), "set_vol_shape")
+
+    def vol_shapes(self, curved):
+        return vol_shapes(self.h, curved)
+
     def vol_warps_candidates(self, curved):
         c = (ctypes.c_int * 3)()
         n = lib().wadg_vol_warps_candidates(self.h, int(curved), c)
@@ -268,6 +277,24 @@ class Context:
         d = self.ops.dim
         fn = getattr(L, f"wadg_euler_update_{d}d" + ("_curved" if curved else ""))
         check(fn(self.h, K, Jq, VqPq, VfPq, fa, fb, fdt, rhsQ, resQ, Q, Qf), "update")
+
+
+MAX_VOL_SHAPES = 5  # WADG_MAX_VOL_SHAPES
+
+
+def shape_label(warps, rows):
+    return str(warps) if rows == 0 else f"{warps}w{rows}r"
+
+
+def vol_shapes(ctx_handle, curved):
+    """[(warps, rows per lane)] of every compiled shape of the volume kernel
+    (wadg_vol_shapes; rows 0 = the default node-to-thread map)"""
+    w = (ctypes.c_int * MAX_VOL_SHAPES)()
+    r = (ctypes.c_int * MAX_VOL_SHAPES)()
+    n = lib().wadg_vol_shapes(ctx_handle, int(curved), w, r)
+    if n < 1:
+        raise WadgError(lib().wadg_last_error().decode())
+    return [(w[k], r[k]) for k in range(n)]
 
 
 def _dp(a):
@@ -406,16 +433,27 @@ class App:
         return list(ms)
 
     def autotune(self, dt, nstages=10):
-        """Pick the volume kernel's CTA shape by timing each compiled one on
-        this app (advances the state: set it afterwards).  Returns
-        (chosen warps per CTA, {warps: ms per volume launch})."""
+        """Pick the volume kernel's shape (warps per CTA and node-to-thread
+        map) by timing each compiled one on this app (advances the state: set
+        it afterwards).  Returns (the chosen shape, {shape: ms per launch});
+        a shape is its warps per CTA ("12") or, for another map than the
+        default, warps and rows per lane ("16w2r")."""
         w = ctypes.c_int()
-        t = (ctypes.c_float * 3)()
+        t = (ctypes.c_float * MAX_VOL_SHAPES)()
         check(lib().wadg_app_autotune(self.h, dt, nstages, ctypes.byref(w), t), "autotune")
         ctx = ctypes.c_void_p(lib().wadg_app_ctx(self.h))
-        cand = (ctypes.c_int * 3)()
-        n = lib().wadg_vol_warps_candidates(ctx, int(self.curved), cand)
-        return w.value, {int(cand[k]): float(t[k]) for k in range(n)}
+        shapes = vol_shapes(ctx, self.curved)
+        rows = lib().wadg_ctx_get_vol_rows(ctx)
+        return shape_label(w.value, rows), {shape_label(a, b): float(t[k]) for k, (a, b) in enumerate(shapes)}
+
+    def vol_shape(self):
+        """(warps, rows) of the volume kernel shape the app's kernels use"""
+        ctx = ctypes.c_void_p(lib().wadg_app_ctx(self.h))
+        return lib().wadg_ctx_get_vol_warps(ctx), lib().wadg_ctx_get_vol_rows(ctx)
+
+    def set_vol_shape(self, warps, rows):
+        ctx = ctypes.c_void_p(lib().wadg_app_ctx(self.h))
+        check(lib().wadg_ctx_set_vol_shape(ctx, int(self.curved), warps, rows), "set_vol_shape")
 
 
 class Solver:

@@ -224,7 +224,7 @@ __device__ __forceinline__ double lambda_dev(const AdjNode<DIM> &s, const Phys &
   double kin = 0.0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) kin = fma(s.vel[d], s.vel[d], kin);
-  const double un = sqrt(kin), c = sqrt(0.5 * P.gamma * s.ibeta);
+  const double un = fsqrt(kin), c = fsqrt(0.5 * P.gamma * s.ibeta);
   if (GRAD) {
     // d|u|/drho = -|u|/rho, d|u|/dm = u/(|u| rho); dc = gamma/(2c) (dp/rho - p/rho^2)
     const double k = 0.5 * P.gamma * rcp(c) * s.irho;
@@ -248,8 +248,8 @@ __device__ __forceinline__ AdjNode<DIM> adj_node(const double *q, int stride, co
   a.beta = s.beta;
   a.lrho = s.lrho;
   a.lbeta = s.lbeta;
-  a.irho = 1.0 / s.rho;
-  a.ibeta = 1.0 / s.beta;
+  a.irho = rcp(s.rho);
+  a.ibeta = rcp(s.beta);
   return a;
 }
 

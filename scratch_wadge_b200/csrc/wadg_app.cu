@@ -488,16 +488,16 @@ int wadg_app_time_kernels(wadg_app *a, double dt, int nstages, float *ms) {
 
 int wadg_app_autotune(wadg_app *a, double dt, int nstages, int *warps, float *times) {
   if (!a || nstages <= 0) return afail(WADG_ERR_INVALID, "invalid argument");
-  int cand[3];
-  const int n = wadg_vol_warps_candidates(a->ctx, a->curved, cand);
+  int cw[WADG_MAX_VOL_SHAPES], cr[WADG_MAX_VOL_SHAPES];
+  const int n = wadg_vol_shapes(a->ctx, a->curved, cw, cr);
   if (n <= 0) return afail(WADG_ERR_UNSUPPORTED, "no volume kernel shapes");
-  int best = cand[0];
+  int best = 0;
   float best_ms = -1.0f;
   // the volume kernel's time, or (volume + surface variant) the volume +
   // surface kernel's
   const bool vs = a->fused == WADG_STAGE_VOLSURF;
   for (int i = 0; i < n; ++i) {
-    int r = wadg_ctx_set_vol_warps(a->ctx, a->curved, cand[i]);
+    int r = wadg_ctx_set_vol_shape(a->ctx, a->curved, cw[i], cr[i]);
     float ms[3] = {0, 0, 0};
     if (!r) r = vs ? wadg_app_time_volsurf(a, dt, 1, ms) : wadg_app_time_kernels(a, dt, 1, ms);
     if (!r) r = vs ? wadg_app_time_volsurf(a, dt, nstages, ms) : wadg_app_time_kernels(a, dt, nstages, ms);
@@ -505,7 +505,7 @@ int wadg_app_autotune(wadg_app *a, double dt, int nstages, int *warps, float *ti
     if (times) times[i] = ms[0] / nstages;
     if (best_ms < 0.0f || ms[0] < best_ms) {
       best_ms = ms[0];
-      best = cand[i];
+      best = i;
     }
   }
   // graphs captured with another shape are stale
@@ -514,8 +514,8 @@ int wadg_app_autotune(wadg_app *a, double dt, int nstages, int *warps, float *ti
       cudaGraphExecDestroy(g);
       g = nullptr;
     }
-  if (warps) *warps = best;
-  return wadg_ctx_set_vol_warps(a->ctx, a->curved, best);
+  if (warps) *warps = cw[best];
+  return wadg_ctx_set_vol_shape(a->ctx, a->curved, cw[best], cr[best]);
 }
 
 int wadg_app_time_stage(wadg_app *a, double dt, int nstages, float *ms) {

@@ -24,6 +24,7 @@ struct wadg_ctx {
   Phys phys;
   cudaStream_t stream;
   int vol_warps = 0;  // warps per CTA of the pair volume kernel; 0 = the default
+  int vol_rows = 0;   // rows per lane of its node-to-thread map; 0 = the default
 };
 
 namespace {
@@ -49,10 +50,10 @@ int after_launch(const char *name) { return cuda_check(cudaGetLastError(), name)
 
 // warps per CTA of the pair-scheduled volume kernel: an even count, as many
 // as fit in 227 KB of shared memory, at most `cap`
-template <int DIM, int N, bool CURVED>
+template <int DIM, int N, bool CURVED, int RR = 0>
 constexpr int volpairsW_fit(int cap) {
-  using C = VolPairsCfg<DIM, N, CURVED, 2>;
-  constexpr size_t per_warp = C::per_elem * VolTile<DIM, N>::G / C::H;
+  using C = VolPairsCfg<DIM, N, CURVED, 2, RR>;
+  constexpr size_t per_warp = C::per_elem * VolTile<DIM, N, RR>::G / C::H;
   constexpr size_t w = (227 * 1024 - C::fixed) / per_warp;
   return w >= (size_t)cap ? cap : (w < 2 ? 2 : (int)(w & ~size_t(1)));
 }
@@ -87,17 +88,59 @@ constexpr int volpairsW_cand(int i) {
   return i == 0 ? W0 : (W0 - 2 * i >= 2 ? W0 - 2 * i : 0);
 }
 
+// The other node-to-thread maps: half and twice the default's lanes per
+// element (about twice and half its rows per lane), each given to the kernels
+// as RR = rows per lane.  A map is a candidate when it has as many lanes as
+// intended (2 to 32), keeps a face node per lane in each warp's face half,
+// pads no more node slots than the default, holds at most 4 rows per lane and
+// fits a CTA of at least 4 warps in shared memory.  (Six rows per lane need
+// more than 255 registers in 3D: 140-530 bytes of spills at every degree.)
+// alt_rows<DIM, N, CURVED, j>(), j = 0 (half the lanes) or 1 (twice): its RR,
+// or 0 when it is no candidate; its warps per CTA: the most that fit, up to 16
+// with at most two rows per lane, else 8 (up to 255 registers per thread).
+template <int DIM, int N, int RR>
+struct NodeMap {  // VolTile's arithmetic, without its static checks
+  static constexpr int Nq = Elem<DIM, N>::Nq;
+  static constexpr int Lraw = RR > 0 ? (Nq + RR - 1) / RR : (Nq + 2) / 3;
+  static constexpr int L = Lraw <= 1 ? 1 : Lraw <= 2 ? 2 : Lraw <= 4 ? 4 : Lraw <= 8 ? 8 : Lraw <= 16 ? 16 : 32;
+  static constexpr int R = (Nq + L - 1) / L;
+  static constexpr int pad = L * R - Nq;
+};
+template <int DIM, int N, bool CURVED, int RR>
+constexpr int alt_warps() {
+  return volpairsW_fit<DIM, N, CURVED, RR>(NodeMap<DIM, N, RR>::R <= 2 ? 16 : 8);
+}
+template <int DIM, int N, bool CURVED, int j>
+constexpr int alt_rows() {
+  constexpr int L0 = NodeMap<DIM, N, 0>::L, Lt = j == 0 ? L0 / 2 : 2 * L0;
+  if constexpr (Lt < 2 || Lt > 32) {
+    return 0;
+  } else {
+    constexpr int RR = (Elem<DIM, N>::Nq + Lt - 1) / Lt;
+    using M = NodeMap<DIM, N, RR>;
+    // (nf1: the smaller face half, the second warp's when there are two)
+    constexpr int nf1 = Elem<DIM, N>::NfqNf / 2;
+    constexpr int faces = nf1 >= M::L ? nf1 : Elem<DIM, N>::NfqNf;
+    if constexpr (M::L != Lt || faces < M::L || M::pad > NodeMap<DIM, N, 0>::pad || M::R > 4) {
+      return 0;
+    } else {
+      constexpr int W = alt_warps<DIM, N, CURVED, RR>();
+      return (W >= 4 && VolPairsCfg<DIM, N, CURVED, W, RR>::smem <= 227 * 1024) ? RR : 0;
+    }
+  }
+}
+
 // SURF: the volume + surface kernel (rhsQf unused; fgeo, mapPq read)
-template <int DIM, int N, bool CURVED, int W, bool SURF = false>
+template <int DIM, int N, bool CURVED, int W, bool SURF = false, int RR = 0>
 int launch_vol_pairs_w(const wadg_ctx *c, int K, const double *vgeo, const double *vfgeo,
                        const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
                        const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
                        const double *Qf, double *rhsQ, double *rhsQf,
                        const double *fgeo = nullptr, const uint32_t *mapPq = nullptr,
                        const int *blist = nullptr, const int *nb = nullptr) {
-  using C = VolPairsCfg<DIM, N, CURVED, W>;
+  using C = VolPairsCfg<DIM, N, CURVED, W, RR>;
   static_assert(C::smem_vol <= 227 * 1024, "pair-scheduled volume kernel does not fit in shared memory");
-  auto kern = vol_pairs_kernel<DIM, N, CURVED, W, SURF>;
+  auto kern = vol_pairs_kernel<DIM, N, CURVED, W, SURF, RR>;
   static wadg_internal::PerDevice<bool> attr;
   if (!attr.here()) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_vol);
@@ -118,6 +161,17 @@ int launch_volsurf(const wadg_ctx *c, int K, const double *vgeo, const double *v
                    const double *nsJ, const double *ntJ, const double *Drq, const double *Dsq,
                    const double *Dtq, const double *VqLq, const double *VfPq, const double *Qf,
                    double *rhsQ, const int *blist = nullptr, const int *nb = nullptr) {
+  constexpr int A0 = alt_rows<DIM, N, CURVED, 0>(), A1 = alt_rows<DIM, N, CURVED, 1>();
+  if constexpr (A0 > 0)
+    if (c->vol_rows == A0)
+      return launch_vol_pairs_w<DIM, N, CURVED, alt_warps<DIM, N, CURVED, A0>(), true, A0>(
+          c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo,
+          mapPq, blist, nb);
+  if constexpr (A1 > 0)
+    if (c->vol_rows == A1)
+      return launch_vol_pairs_w<DIM, N, CURVED, alt_warps<DIM, N, CURVED, A1>(), true, A1>(
+          c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, nullptr, fgeo,
+          mapPq, blist, nb);
   constexpr int W1 = volpairsW_cand<DIM, N, CURVED>(1), W2 = volpairsW_cand<DIM, N, CURVED>(2);
   if (W1 && c->vol_warps == W1)
     return launch_vol_pairs_w<DIM, N, CURVED, (W1 ? W1 : 2), true>(
@@ -138,6 +192,15 @@ int launch_vol_pairs(const wadg_ctx *c, int K, const double *vgeo, const double 
                      const double *nrJ, const double *nsJ, const double *ntJ, const double *Drq,
                      const double *Dsq, const double *Dtq, const double *VqLq, const double *VfPq,
                      const double *Qf, double *rhsQ, double *rhsQf) {
+  constexpr int A0 = alt_rows<DIM, N, CURVED, 0>(), A1 = alt_rows<DIM, N, CURVED, 1>();
+  if constexpr (A0 > 0)
+    if (c->vol_rows == A0)
+      return launch_vol_pairs_w<DIM, N, CURVED, alt_warps<DIM, N, CURVED, A0>(), false, A0>(
+          c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf);
+  if constexpr (A1 > 0)
+    if (c->vol_rows == A1)
+      return launch_vol_pairs_w<DIM, N, CURVED, alt_warps<DIM, N, CURVED, A1>(), false, A1>(
+          c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, Qf, rhsQ, rhsQf);
   constexpr int W1 = volpairsW_cand<DIM, N, CURVED>(1), W2 = volpairsW_cand<DIM, N, CURVED>(2);
   if (W1 && c->vol_warps == W1)
     return launch_vol_pairs_w<DIM, N, CURVED, (W1 ? W1 : 2)>(c, K, vgeo, vfgeo, nrJ, nsJ, ntJ, Drq,
@@ -154,6 +217,24 @@ int vol_warps_candidates(int *out) {
   int n = 0;
   for (int i = 0; i < 3; ++i)
     if (int w = volpairsW_cand<DIM, N, CURVED>(i)) out[n++] = w;
+  return n;
+}
+
+// every compiled (warps, rows) shape: the default map's warps, then the
+// other maps (rows > 0)
+template <int DIM, int N, bool CURVED>
+int vol_shapes(int *warps, int *rows) {
+  int n = vol_warps_candidates<DIM, N, CURVED>(warps);
+  for (int i = 0; i < n; ++i) rows[i] = 0;
+  constexpr int A0 = alt_rows<DIM, N, CURVED, 0>(), A1 = alt_rows<DIM, N, CURVED, 1>();
+  if constexpr (A0 > 0) {
+    warps[n] = alt_warps<DIM, N, CURVED, A0>();
+    rows[n++] = A0;
+  }
+  if constexpr (A1 > 0) {
+    warps[n] = alt_warps<DIM, N, CURVED, A1>();
+    rows[n++] = A1;
+  }
   return n;
 }
 
@@ -211,9 +292,9 @@ int update_grid(int K, int *grid) {
 }
 
 // the launch shape of one kernel for K elements (wadg_kernel_shape)
-template <int DIM, int N, bool CURVED, int W>
+template <int DIM, int N, bool CURVED, int W, int RR = 0>
 void vol_shape(int K, int *E, int *grid) {
-  using C = VolPairsCfg<DIM, N, CURVED, W>;
+  using C = VolPairsCfg<DIM, N, CURVED, W, RR>;
   *E = C::E;
   *grid = persistent_grid(K, C::E, C::smem_vol);
 }
@@ -221,6 +302,14 @@ void vol_shape(int K, int *E, int *grid) {
 template <int DIM, int N, bool CURVED>
 int kernel_shape(const wadg_ctx *c, int kernel, int K, int *E, int *grid) {
   constexpr int W1 = volpairsW_cand<DIM, N, CURVED>(1), W2 = volpairsW_cand<DIM, N, CURVED>(2);
+  constexpr int A0 = alt_rows<DIM, N, CURVED, 0>(), A1 = alt_rows<DIM, N, CURVED, 1>();
+  if ((kernel == WADG_KERNEL_VOL || kernel == WADG_KERNEL_VOLSURF) && c->vol_rows) {
+    if constexpr (A0 > 0)
+      if (c->vol_rows == A0) vol_shape<DIM, N, CURVED, alt_warps<DIM, N, CURVED, A0>(), A0>(K, E, grid);
+    if constexpr (A1 > 0)
+      if (c->vol_rows == A1) vol_shape<DIM, N, CURVED, alt_warps<DIM, N, CURVED, A1>(), A1>(K, E, grid);
+    return WADG_OK;
+  }
   switch (kernel) {
     case WADG_KERNEL_VOL:
       if (W1 && c->vol_warps == W1) vol_shape<DIM, N, CURVED, (W1 ? W1 : 2)>(K, E, grid);
@@ -494,8 +583,35 @@ int wadg_ctx_set_vol_warps(wadg_ctx *ctx, int curved, int warps) {
     if (!ok) return fail(WADG_ERR_INVALID, "%d warps per CTA is not a compiled shape", warps);
   }
   ctx->vol_warps = warps;
+  ctx->vol_rows = 0;
   return WADG_OK;
 }
+
+int wadg_vol_shapes(const wadg_ctx *ctx, int curved, int *warps, int *rows) {
+  if (!ctx || !warps || !rows) return -fail(WADG_ERR_INVALID, "null argument");
+  const wadg_ctx *c = ctx;
+  if (curved) {
+    WADG_DISPATCH(c, return (vol_shapes<D_, N_, true>(warps, rows)));
+  } else {
+    WADG_DISPATCH(c, return (vol_shapes<D_, N_, false>(warps, rows)));
+  }
+}
+
+int wadg_ctx_set_vol_shape(wadg_ctx *ctx, int curved, int warps, int rows) {
+  if (!ctx) return fail(WADG_ERR_INVALID, "null context");
+  if (rows == 0) return wadg_ctx_set_vol_warps(ctx, curved, warps);
+  int w[WADG_MAX_VOL_SHAPES], r[WADG_MAX_VOL_SHAPES];
+  const int n = wadg_vol_shapes(ctx, curved, w, r);
+  for (int i = 0; i < n; ++i)
+    if (w[i] == warps && r[i] == rows) {
+      ctx->vol_warps = warps;
+      ctx->vol_rows = rows;
+      return WADG_OK;
+    }
+  return fail(WADG_ERR_INVALID, "%d warps x %d rows per lane is not a compiled shape", warps, rows);
+}
+
+int wadg_ctx_get_vol_rows(const wadg_ctx *ctx) { return ctx ? ctx->vol_rows : -1; }
 
 int wadg_ctx_get_vol_warps(const wadg_ctx *ctx) { return ctx ? ctx->vol_warps : -1; }
 

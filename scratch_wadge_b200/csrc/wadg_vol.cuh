@@ -32,9 +32,13 @@
 
 namespace wadg {
 
-template <int DIM, int N> struct VolTile {
+// Node-to-thread map: L lanes per element, R rows per lane.  RR = 0: about
+// three rows per lane (L = the power of two >= Nq/3); RR > 0: about RR rows
+// (an autotuner candidate where it pads less, e.g. 2D N=4: Nq = 16 fills
+// L = 4 x 4 or 8 x 2 exactly, against 8 x 3 = 24 slots by default)
+template <int DIM, int N, int RR = 0> struct VolTile {
   using El = Elem<DIM, N>;
-  static constexpr int Lraw = (El::Nq + 2) / 3;
+  static constexpr int Lraw = RR > 0 ? (El::Nq + RR - 1) / RR : (El::Nq + 2) / 3;
   static constexpr int L = Lraw <= 1 ? 1 : Lraw <= 2 ? 2 : Lraw <= 4 ? 4 : Lraw <= 8 ? 8 : Lraw <= 16 ? 16 : 32;
   static constexpr int R = (El::Nq + L - 1) / L;
   static constexpr int G = 32 / L;  // elements per warp group
@@ -46,10 +50,10 @@ template <int DIM, int N> struct VolTile {
   __host__ __device__ static constexpr int f0(int h) { return h ? nf0 : 0; }
 };
 
-template <int DIM, int N, bool CURVED, int W>
+template <int DIM, int N, bool CURVED, int W, int RR = 0>
 struct VolPairsCfg {
   using El = Elem<DIM, N>;
-  using T = VolTile<DIM, N>;
+  using T = VolTile<DIM, N, RR>;
   static constexpr int H = T::H;                      // warps per element group
   static constexpr int threads = 32 * W;
   static constexpr int E = (W / H) * T::G;            // elements per batch
@@ -78,11 +82,11 @@ struct VolPairsCfg {
 };
 
 // Shared-memory carve-up and the two phases common to both kernels.
-template <int DIM, int N, bool CURVED, int W>
+template <int DIM, int N, bool CURVED, int W, int RR = 0>
 struct VolPairs {
   using El = Elem<DIM, N>;
-  using T = VolTile<DIM, N>;
-  using C = VolPairsCfg<DIM, N, CURVED, W>;
+  using T = VolTile<DIM, N, RR>;
+  using C = VolPairsCfg<DIM, N, CURVED, W, RR>;
   static constexpr int Nq = El::Nq, NF = El::NfqNf, Nfq = El::Nfq, NN = El::NN, NS = El::NS;
   static constexpr int Nf = El::Nfields, NG = El::Nvgeo, L = T::L, R = T::R, G = T::G, E = C::E;
   static constexpr int SE = C::SE, SA = C::SA, SN = C::SN, H = C::H;
@@ -413,7 +417,7 @@ struct VolPairs {
 // mapPq; Qf is only read, so every element's traces are final) and lifts
 // them into its rows; rhsQ <- the whole right-hand side the surface kernel
 // would leave, rhsQf is not written (fgeo and mapPq unused when false)
-template <int DIM, int N, bool CURVED, int W, bool SURF = false>
+template <int DIM, int N, bool CURVED, int W, bool SURF = false, int RR = 0>
 __global__ void __launch_bounds__(32 * W, 1)
 vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
                  const double *__restrict__ nrJ, const double *__restrict__ nsJ,
@@ -424,7 +428,7 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
                  double *__restrict__ rhsQf, Phys P, const double *__restrict__ fgeo = nullptr,
                  const uint32_t *__restrict__ mapPq = nullptr,
                  const int *__restrict__ blist = nullptr, const int *__restrict__ nblist = nullptr) {
-  using V = VolPairs<DIM, N, CURVED, W>;
+  using V = VolPairs<DIM, N, CURVED, W, RR>;
   constexpr int Nq = V::Nq, NF = V::NF, Nf = V::Nf, R = V::R, L = V::L, E = V::E, H = V::H;
   extern __shared__ double smem[];
   V v(smem);

@@ -122,7 +122,7 @@ def main(argv=None):
     if kernels:
         out["kernel_ms"] = kernels
     if warps is not None:
-        out["vol_warps"] = warps
+        out["vol_shape"] = warps
     if kind in ("vortex", "density_wave", "constant"):
         out["l2_error"] = IC.l2_error(geo, Q, IC.exact_state(geo, kind, dt * nsteps, args.gamma))
     if args.datadir:

@@ -71,11 +71,11 @@ def state(geo, curved, seed):
 
 
 def shapes(ctx, curved, K):
-    """per volume CTA shape: (warps, E, grid at K)"""
+    """per volume kernel shape: ((warps, rows), E, grid at K)"""
     out = []
-    for w in ctx.vol_warps_candidates(curved):
-        ctx.set_vol_warps(curved, w)
-        out.append((w,) + ctx.shape("vol", curved, K))
+    for w, r in ctx.vol_shapes(curved):
+        ctx.set_vol_shape(curved, w, r)
+        out.append(((w, r),) + ctx.shape("vol", curved, K))
     ctx.set_vol_warps(curved, 0)
     return out
 
@@ -104,11 +104,11 @@ def test_kernels_over_several_batches_per_cta(cuda, dim, N, curved):
     # the update of these rough states stays physical
     dt = IC.time_step(geo, 0.1, N, nsteps=1, wave_speed=IC.max_wave_speed(st["Q"]))[0]
 
-    # volume kernel, every compiled CTA shape
+    # volume kernel, every compiled shape
     for w, E, g in sh:
         K = Kvol[w]
         assert (K + E - 1) // E > 2 * g and K % E, (w, E, g, K)
-        d.ctx.set_vol_warps(curved, w)
+        d.ctx.set_vol_shape(curved, *w)
         s = d.put(st)
         d.ctx.vol(curved, K, *[d.g[n].data_ptr() for n in ("vgeo", "vfgeo", "nrJ", "nsJ", "ntJ", "Drq",
                                                            "Dsq", "Dtq", "VqLq", "VfPq")],
