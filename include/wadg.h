@@ -304,13 +304,15 @@ int wadg_entropy_rhs(wadg_ctx *ctx, int K, int curved, const double *wq,
 
 /* ------------------------------------------------------------ fused stage
  * One LSRK stage -- vol, surf and update of the kernels above -- in a single
- * launch (rk_step, euler.c:3610-3666, with rhsQf and the volume RHS kept on
- * chip).  No single-kernel counterpart in the reference.  The entropy-
- * projected state is read from (rhsQ_in, Qf_in) and written to (rhsQ_out,
- * Qf_out), which must be distinct buffers (a neighbour's trace of the current
- * stage is still being read while the next stage's is written); Q and resQ
- * are updated in place.  curved = 0: Euler3Daffine / euler_vol_2d algebra;
- * 1: Euler3D curved / WADG. */
+ * launch (rk_step, euler.c:3610-3666, with rhsQf kept on chip and each group
+ * of 8 elements updated as soon as its right-hand side is complete).  No
+ * single-kernel counterpart in the reference.  The entropy-projected state
+ * is read from (rhsQ_in, Qf_in); rhsQ_out receives the RHS and then the next
+ * stage's state, Qf_out the next traces.  Qf_out must differ from Qf_in
+ * (WADG_ERR_INVALID otherwise: a neighbour's trace of the current stage is
+ * still being read while the next stage's is written); rhsQ_out may equal
+ * rhsQ_in.  Q and resQ are updated in place.  curved = 0: Euler3Daffine /
+ * euler_vol_2d algebra; 1: Euler3D curved / WADG. */
 int wadg_euler_stage_3d(wadg_ctx *ctx, int K, int curved, const double *vgeo,
                         const double *vfgeo, const double *fgeo,
                         const uint32_t *mapPq, const double *nrJ,

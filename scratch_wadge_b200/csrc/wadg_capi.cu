@@ -15,6 +15,7 @@
 #include "wadg_diag.cuh"
 #include "wadg_surf_mma.cuh"
 #include "wadg_update_mma.cuh"
+#include "wadg_stage.cuh"
 #include "wadg_vol.cuh"
 
 using namespace wadg;
@@ -245,17 +246,18 @@ int launch_stage(const wadg_ctx *c, int K, const double *vgeo, const double *vfg
                  const double *VqLq, const double *VfPq, const double *VqPq, const double *Jq,
                  double fa, double fb, double fdt, const double *uq, const double *uf, double *Q,
                  double *resQ, double *uq_out, double *uf_out) {
-  constexpr int W = volpairsW<DIM, N, CURVED>();
+  if (uf_out == uf) return fail(WADG_ERR_INVALID, "stage: uf_out must not be uf");
+  constexpr int W = stage_warps<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>();
   using C = VolPairsCfg<DIM, N, CURVED, W>;
   auto kern = stage_kernel<DIM, N, CURVED, W>;
   static wadg_internal::PerDevice<bool> attr;
   if (!attr.here()) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_vol);
     if (e != cudaSuccess) return cuda_check(e, "stage kernel smem attribute");
     attr.here() = true;
   }
-  const int grid = persistent_grid(K, C::E, C::smem);
-  kern<<<grid, C::threads, C::smem, c->stream>>>(K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq,
+  const int grid = persistent_grid(K, C::E, C::smem_vol);
+  kern<<<grid, C::threads, C::smem_vol, c->stream>>>(K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq,
                                                   Dsq, Dtq, VqLq, VfPq, VqPq, Jq, fa, fb, fdt, uq,
                                                   uf, Q, resQ, uq_out, uf_out, c->phys);
   return after_launch("stage kernel");
@@ -331,9 +333,9 @@ int kernel_shape(const wadg_ctx *c, int kernel, int K, int *E, int *grid) {
     case WADG_KERNEL_ADJ_PAIRS:
       return wadg_internal::adj_pairs_shape(DIM, N, CURVED, K, E, grid);
     case WADG_KERNEL_STAGE: {
-      using C = VolPairsCfg<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>;
+      using C = VolPairsCfg<DIM, N, CURVED, stage_warps<DIM, N, CURVED, volpairsW<DIM, N, CURVED>()>()>;
       *E = C::E;
-      *grid = persistent_grid(K, C::E, C::smem);
+      *grid = persistent_grid(K, C::E, C::smem_vol);
       return WADG_OK;
     }
   }

@@ -136,6 +136,11 @@ __device__ __forceinline__ void mtile_store(double *Y, int mt, int lane, const d
   }
 }
 
+// the CTA-wide barrier (the update kernel: one group per CTA)
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
 // the LSRK operands of a lane's two (node, element) pairs of m-tile mt
 template <int Nq, int Nf>
 __device__ __forceinline__ void load_lsrk(const double *__restrict__ resQ,
@@ -162,19 +167,23 @@ __device__ __forceinline__ void load_lsrk(const double *__restrict__ resQ,
 // zero): r = M^{-1} rhs, the LSRK update of resQ and Q, v = V(Q) (WADG: the
 // weight-adjusted projection of v), the next traces U(VfPq v) -> Qf_out and
 // U(VqPq v) -> rhsQ_out.  res0/q0/Jv hold the LSRK operands of the warp's
-// first m-tile (load_lsrk), loaded early by the caller.  Every warp of the
-// CTA calls this; it ends with the output stores (the caller synchronises
-// before X or Y are written again).
-template <int DIM, int N, bool CURVED>
+// first m-tile (load_lsrk), loaded early by the caller; PRE = false: each
+// m-tile loads its own after its product (fewer registers live across the
+// MMAs; the caller's res0/q0/Jv are scratch).  The UW warps that share the
+// group (warp = 0 .. UW-1 among them) call this; `sync` is their barrier.  It
+// ends with the output stores (the caller synchronises before X or Y are
+// written again).
+template <int DIM, int N, bool CURVED, int UW = UpdMmaCfg<DIM, N, CURVED>::WARPS,
+          bool PRE = true, typename SyncF = CtaSync>
 __device__ __forceinline__ void update_group(
     int k0, int ne, int warp, int lane, double *X, double *Y, const double *__restrict__ Jq,
     const double *__restrict__ VqPq, const double *__restrict__ VfPq, double fa, double fb,
     double fdt, double *__restrict__ resQ, double *__restrict__ Q, double *__restrict__ rhsQ_out,
     double *__restrict__ Qf_out, const Phys &P, double (*res0)[DIM + 2], double (*q0)[DIM + 2],
-    double *Jv, const double *__restrict__ dtK = nullptr) {
+    double *Jv, const double *__restrict__ dtK = nullptr, SyncF sync = SyncF()) {
   using C = UpdMmaCfg<DIM, N, CURVED>;
   constexpr int Nq = C::Nq, NF = C::NF, Nf = C::Nf, EW = C::EW, KS = C::KS, LD = C::LD,
-                MQ = C::MQ, MO = C::MO, W = C::WARPS;
+                MQ = C::MQ, MO = C::MO, W = UW;
   bool ev[2];
   double dte[2];  // the step of the lane's two elements: fdt, or per element (dtK)
 #pragma unroll
@@ -192,17 +201,18 @@ __device__ __forceinline__ void update_group(
       mtile_gemm<KS, Nf, LD>(a, X, lane, D);
       mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, -2.0, Jq, k0, ne);
     }
-    __syncthreads();
+    sync();
     R = Y;
   }
   // the update proper; V(U) goes to the other buffer (affine: Y; WADG: X,
   // scaled by J for the projection that follows)
   double *Vb = CURVED ? X : Y;
   for (int mt = warp; mt < MQ; mt += W) {
-    if (mt != warp) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, mt, lane, res0, q0, Jv);
+    if (PRE && mt != warp) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, mt, lane, res0, q0, Jv);
     const int m = mt * 8 + (lane >> 2);
     load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
     mtile_gemm<KS, Nf, LD>(a, R, lane, D);
+    if (!PRE) load_lsrk<Nq, Nf>(resQ, Q, Jq, k0, ne, mt, lane, res0, q0, Jv);
     if (m < Nq) {
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -231,7 +241,7 @@ __device__ __forceinline__ void update_group(
       }
     }
   }
-  __syncthreads();
+  sync();
   const double *Xo = Y;  // the operand of the output projection
   if (CURVED) {
     // v~ = VqPq((VqPq(v J)) / J): X -> Y -> X
@@ -240,13 +250,13 @@ __device__ __forceinline__ void update_group(
       mtile_gemm<KS, Nf, LD>(a, X, lane, D);
       mtile_store<Nq, Nf, LD, true>(Y, mt, lane, D, 1.0, Jq, k0, ne);
     }
-    __syncthreads();
+    sync();
     for (int mt = warp; mt < MQ; mt += W) {
       load_afrag<KS, Nq>(VqPq, Nq, Nq, mt, lane, a);
       mtile_gemm<KS, Nf, LD>(a, Y, lane, D);
       mtile_store<Nq, Nf, LD, false>(X, mt, lane, D, 1.0, Jq, k0, ne);
     }
-    __syncthreads();
+    sync();
     Xo = X;
   }
 
@@ -275,24 +285,26 @@ __device__ __forceinline__ void update_group(
 
 // stage the rhs block [e][f][node] of a group as X[node][f*8 + e] (columns of
 // elements past the end get 0): loads first, then the barrier that frees X,
-// then the stores; `between` runs after the loads are issued
-template <int Nq, int Nf, int LD, int THREADS, typename F>
-__device__ __forceinline__ void stage_rhs(const double *__restrict__ rhs, int k0, int ne, double *X,
-                                          F between) {
+// then the stores; `between` runs after the loads are issued.  Threads tid =
+// 0 .. THREADS-1 with the barrier `sync`; CG: the loads bypass L1 (the block
+// was written earlier in the same launch, by other threads)
+template <int Nq, int Nf, int LD, int THREADS, bool CG = false, typename F, typename SyncF = CtaSync>
+__device__ __forceinline__ void stage_rhs(const double *rhs, int k0, int ne, double *X, F between,
+                                          int tid = threadIdx.x, SyncF sync = SyncF()) {
   constexpr int EW = 8, TOT = EW * Nf * Nq, IT = (TOT + THREADS - 1) / THREADS;
   const double *src = rhs + (size_t)k0 * Nf * Nq;
   const int lim = ne * Nf * Nq;
   double v[IT];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
-    const int t = threadIdx.x + THREADS * it;
-    v[it] = t < lim ? src[t] : 0.0;
+    const int t = tid + THREADS * it;
+    v[it] = t < lim ? (CG ? __ldcg(src + t) : __ldg(src + t)) : 0.0;
   }
   between();
-  __syncthreads();  // the previous group's last reads of X and Y are done
+  sync();  // the previous group's last reads of X and Y are done
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
-    const int t = threadIdx.x + THREADS * it;
+    const int t = tid + THREADS * it;
     if (t < TOT) {
       const int e = t / (Nf * Nq), rem = t - e * (Nf * Nq);
       const int f = rem / Nq, n = rem - f * Nq;

@@ -509,171 +509,4 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
   }
 }
 
-// ---------------------------------------------------------------- fused stage
-// One LSRK stage in one launch: volume pairs, surface flux + LF penalty, lift,
-// inverse mass, LSRK update and entropy projection -- rk_step of the reference
-// (euler.c:3610-3666: euler_vol_3d, euler_surf_3d, euler_update_3d or the
-// curved / 2D counterparts) with the intermediates (rhsQf, the volume RHS)
-// kept in shared memory.  The entropy-projected state is read from (uq, uf)
-// and written to (uq_out, uf_out), distinct buffers, because the surface flux
-// of an element reads its neighbours' traces of the current stage while other
-// CTAs already write the next stage's.  Q and resQ are updated in place (each
-// element touches only its own).
-template <int DIM, int N, bool CURVED, int W>
-__global__ void __launch_bounds__(32 * W, 1)
-stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ vfgeo,
-             const double *__restrict__ fgeo, const uint32_t *__restrict__ mapPq,
-             const double *__restrict__ nrJ, const double *__restrict__ nsJ,
-             const double *__restrict__ ntJ, const double *__restrict__ Drq,
-             const double *__restrict__ Dsq, const double *__restrict__ Dtq,
-             const double *__restrict__ VqLq, const double *__restrict__ VfPq,
-             const double *__restrict__ VqPq, const double *__restrict__ Jq, double fa,
-             double fb, double fdt, const double *__restrict__ uq, const double *__restrict__ uf,
-             double *__restrict__ Q, double *__restrict__ resQ, double *__restrict__ uq_out,
-             double *__restrict__ uf_out, Phys P) {
-  using V = VolPairs<DIM, N, CURVED, W>;
-  using El = Elem<DIM, N>;
-  constexpr int Nq = V::Nq, NF = V::NF, Nf = V::Nf, R = V::R, L = V::L, E = V::E, H = V::H;
-  constexpr int SE = V::SE, SA = V::SA, NFG = El::Nfgeo;
-  extern __shared__ double smem[];
-  V v(smem);
-  v.load_tables(nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq);
-  // as in vol_pairs_kernel, an element group's warps synchronise only among
-  // themselves after the tables: every phase below touches only the group's
-  // own elements' shared memory
-  constexpr int G = V::G, GT = 32 * H;
-  const int q = (threadIdx.x >> 5) / H, tid = threadIdx.x - q * GT, nth = GT, e0 = q * G;
-  auto gsync = [&] {
-    if (H == 1)
-      __syncwarp();
-    else
-      asm volatile("bar.sync %0, %1;\n" ::"r"(1 + q), "r"(GT) : "memory");
-  };
-  __syncthreads();  // the tables are shared by every group
-
-  for (int k0 = blockIdx.x * E; k0 < K; k0 += gridDim.x * E) {
-    if (k0 + e0 >= K) break;  // the group's elements all lie past the end
-    gsync();
-    v.prologue_range(K, k0, e0, G, tid, nth, vgeo, vfgeo, uq, uf, P, nullptr);
-    gsync();
-    double acc[R][Nf];
-    v.pairs(acc, P);
-    gsync();
-
-    // ---- surface: sfS = rhsQf + 1/2 F_S(u-,u+).nJ - tau/4 max(lam) sJ (u+ - u-)
-    // over the face accumulators, then the lift rows += VqLq sfS
-    v.template surface<GT>(K, k0, e0, tid, fgeo, mapPq, uf, P);
-    gsync();
-    v.lift(acc);
-    v.park_rows(acc);  // the state block is free after the surface phase
-    gsync();
-    if (v.h == 0) {
-      double *rowbuf = v.sSt + v.e * SE;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int i = v.l + L * r;
-        if (i < Nq) {
-#pragma unroll
-          for (int q = 0; q < Nf; ++q)  // full RHS row
-            rowbuf[q * Nq + i] = H == 2 ? rowbuf[q * Nq + i] + acc[r][q] : acc[r][q];
-        }
-      }
-    }
-    gsync();
-
-    // ---- update (Euler3Daffine.okl:555-773 / Euler3D.okl:2527-2884):
-    // staging per element in its state block: [0] rhs, [1] sA, [2] sB
-    auto blk = [&](int ee, int which) { return v.sSt + ee * SE + which * Nf * Nq; };
-    auto matvec = [&](const double *Op, int ld, int row, const double *X, double *out) {
-#pragma unroll
-      for (int q = 0; q < Nf; ++q) out[q] = 0.0;
-      for (int j = 0; j < Nq; ++j) {
-        const double w = __ldg(Op + row + j * ld);
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) out[q] = fma(w, X[q * Nq + j], out[q]);
-      }
-    };
-    if (CURVED) {
-      for (int t = tid; t < G * Nq; t += nth) {
-        const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
-        if (k >= K) continue;
-        double r[Nf];
-        matvec(VqPq, Nq, i, blk(ee, 0), r);
-        const double Jqi = Jq[(size_t)k * Nq + i];
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) blk(ee, 1)[q * Nq + i] = -2.0 * r[q] / Jqi;
-      }
-      gsync();
-    }
-    for (int t = tid; t < G * Nq; t += nth) {
-      const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
-      if (k >= K) continue;
-      const double Jqi = Jq[(size_t)k * Nq + i];
-      double r[Nf], U[Nf], Vv[Nf];
-      if (CURVED) {
-        matvec(VqPq, Nq, i, blk(ee, 1), r);
-      } else {
-        matvec(VqPq, Nq, i, blk(ee, 0), r);
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) r[q] = -2.0 * r[q] / Jqi;
-      }
-      const size_t id = (size_t)k * Nq * Nf + i;
-#pragma unroll
-      for (int q = 0; q < Nf; ++q) {
-        const double res = fa * resQ[id + q * Nq] + fdt * r[q];
-        resQ[id + q * Nq] = res;
-        U[q] = Q[id + q * Nq] + fb * res;
-        Q[id + q * Nq] = U[q];
-      }
-      VU<DIM>(U, Vv, P);
-#pragma unroll
-      for (int q = 0; q < Nf; ++q) blk(ee, 2)[q * Nq + i] = CURVED ? Vv[q] * Jqi : Vv[q];
-    }
-    gsync();
-    int src = 2;  // block holding the projected entropy variables' source
-    if (CURVED) {
-      // weight-adjusted projection VqPq((VqPq (v J)) / J)
-      for (int t = tid; t < G * Nq; t += nth) {
-        const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
-        if (k >= K) continue;
-        double r[Nf];
-        matvec(VqPq, Nq, i, blk(ee, 2), r);
-        const double Jqi = Jq[(size_t)k * Nq + i];
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) blk(ee, 1)[q * Nq + i] = r[q] / Jqi;
-      }
-      gsync();
-      for (int t = tid; t < G * Nq; t += nth) {
-        const int ee = e0 + t / Nq, i = t % Nq, k = k0 + ee;
-        if (k >= K) continue;
-        double r[Nf];
-        matvec(VqPq, Nq, i, blk(ee, 1), r);
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) blk(ee, 0)[q * Nq + i] = r[q];
-      }
-      gsync();
-      src = 0;
-    }
-    for (int t = tid; t < G * (NF + Nq); t += nth) {
-      const int ee = e0 + t / (NF + Nq), n = t % (NF + Nq), k = k0 + ee;
-      if (k >= K) continue;
-      double Vv[Nf], U[Nf];
-      if (n < NF) {
-        matvec(VfPq, NF, n, blk(ee, src), Vv);
-        UV<DIM>(Vv, U, P);
-        double *out = uf_out + (size_t)k * NF * Nf + n;
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) out[q * NF] = U[q];
-      } else {
-        const int i = n - NF;
-        matvec(VqPq, Nq, i, blk(ee, src), Vv);
-        UV<DIM>(Vv, U, P);
-        double *out = uq_out + (size_t)k * Nq * Nf + i;
-#pragma unroll
-        for (int q = 0; q < Nf; ++q) out[q * Nq] = U[q];
-      }
-    }
-  }
-}
-
 }  // namespace wadg
