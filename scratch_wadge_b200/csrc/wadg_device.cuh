@@ -242,6 +242,21 @@ namespace wadg {
 // The branch test reuses f = (a-b)/(a+b), which the series needs anyway.
 // Must be called by all 32 lanes of the warp.
 __device__ __forceinline__ double polyF2(double u) { return fma(fma(u, 1.0 / 5.0, 1.0 / 3.0), u, 1.0); }
+// 2 polyF2(u) and 2 polyF(u) with the factor 2 in the coefficients: scaling
+// by 2 is exact and commutes with rounding, so these are the same bits as
+// 2.0 * poly, one multiplication fewer where the result multiplies isb
+__device__ __forceinline__ double polyF2x2(double u) { return fma(fma(u, 2.0 / 5.0, 2.0 / 3.0), u, 2.0); }
+__device__ __forceinline__ double polyFx2(double u) {
+  double p = 2.0 / 17.0;
+  p = fma(p, u, 2.0 / 15.0);
+  p = fma(p, u, 2.0 / 13.0);
+  p = fma(p, u, 2.0 / 11.0);
+  p = fma(p, u, 2.0 / 9.0);
+  p = fma(p, u, 2.0 / 7.0);
+  p = fma(p, u, 2.0 / 5.0);
+  p = fma(p, u, 2.0 / 3.0);
+  return fma(p, u, 2.0);
+}
 __device__ __forceinline__ double polyG2(double u) { return fma(fma(u, -4.0 / 45.0, -1.0 / 3.0), u, 1.0); }
 
 template <int DIM>
@@ -308,13 +323,13 @@ __device__ __forceinline__ void ecflux_n_warp_hR(const NodeState<DIM> (&a)[R], c
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       rl[r] = hsr[r] * polyG2(ur[r]);
-      ibl[r] = 2.0 * isb[r] * polyF2(ub[r]);
+      ibl[r] = isb[r] * polyF2x2(ub[r]);
     }
   } else {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       rl[r] = (ur[r] < 1e-2) ? hsr[r] * polyG(ur[r]) : dr[r] * rcp(a[r].lrho - b.lrho);
-      ibl[r] = (ub[r] < 1e-2) ? 2.0 * isb[r] * polyF(ub[r]) : (a[r].lbeta - b.lbeta) * rcp(db[r]);
+      ibl[r] = (ub[r] < 1e-2) ? isb[r] * polyFx2(ub[r]) : (a[r].lbeta - b.lbeta) * rcp(db[r]);
     }
   }
 #pragma unroll
