@@ -179,6 +179,22 @@ def test_fused_stage_rejects_aliasing(cuda):
         d.stage(s, {"rhsQ": s["rhsQ"], "Qf": s["Qf"]}, IC.RK4A[1], IC.RK4B[1], c.dt)
 
 
+@pytest.mark.parametrize("name", ["tg3d_affine_N3", "dw3d_curved_N4", "vortex2d_curved_N3"])
+def test_fused_stage_state_in_place(cuda, name):
+    """the stage's state buffer may be both input and output (each element's
+    own state is read before its RHS and next state are written); only the
+    traces need a second buffer"""
+    c = Case(name)
+    d = Dev(cuda, c.geo, c.curved)
+    s = d.put(c.state())
+    out = {"rhsQ": s["rhsQ"], "Qf": cuda.empty_like(s["Qf"])}
+    d.stage(s, out, IC.RK4A[1], IC.RK4B[1], c.dt)
+    d.sync()
+    assert rel(s["rhsQ"].cpu().numpy(), c.z["upd_rhsQ"]) < RTOL
+    assert rel(out["Qf"].cpu().numpy(), c.z["upd_Qf"]) < RTOL
+    assert rel(s["Q"].cpu().numpy(), c.z["upd_Q"]) < RTOL
+
+
 @pytest.mark.parametrize("name", golden_names())
 def test_fused_and_three_kernel_paths_agree(cuda, name):
     c = Case(name)
