@@ -833,8 +833,9 @@ int wadg_euler_stage_3d(wadg_ctx *c, int K, int curved, const double *vgeo, cons
   if (any_null({vgeo, fgeo, mapPq, nrJ, nsJ, ntJ, Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq, rhsQ_in,
                 Qf_in, Q, resQ, rhsQ_out, Qf_out}) || (curved && !vfgeo))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  if (rhsQ_in == rhsQ_out || Qf_in == Qf_out)
-    return fail(WADG_ERR_INVALID, "stage output buffers must not alias the inputs");
+  // the state may be updated in place; the traces need a second buffer
+  if (Qf_in == Qf_out)
+    return fail(WADG_ERR_INVALID, "stage: Qf_out must not be Qf_in");
   if (curved)
     WADG_DISPATCH(c, return (launch_stage<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
                                                          ntJ, Drq, Dsq, Dtq, VqLq, VfPq, VqPq, Jq,
@@ -893,8 +894,9 @@ int wadg_euler_stage_2d(wadg_ctx *c, int K, int curved, const double *vgeo, cons
   if (any_null({vgeo, fgeo, mapPq, nrJ, nsJ, Drq, Dsq, VqLq, VfPq, VqPq, Jq, rhsQ_in, Qf_in, Q,
                 resQ, rhsQ_out, Qf_out}) || (curved && !vfgeo))
     return fail(WADG_ERR_INVALID, "null pointer argument");
-  if (rhsQ_in == rhsQ_out || Qf_in == Qf_out)
-    return fail(WADG_ERR_INVALID, "stage output buffers must not alias the inputs");
+  // the state may be updated in place; the traces need a second buffer
+  if (Qf_in == Qf_out)
+    return fail(WADG_ERR_INVALID, "stage: Qf_out must not be Qf_in");
   if (curved)
     WADG_DISPATCH(c, return (launch_stage<D_, N_, true>(c, K, vgeo, vfgeo, fgeo, mapPq, nrJ, nsJ,
                                                          nullptr, Drq, Dsq, nullptr, VqLq, VfPq,
