@@ -131,7 +131,7 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
     if (PRE) prefetch_group(knext);  // the next batch's traces, during the pairs
     if (vact) {
       double acc[R][Nf];
-      v.pairs(acc, P);
+      v.all_pairs(acc, P);
       gsync();
       v.template surface<GT>(K, k0, q * G, tq, fgeo, mapPq, uf, P);
       gsync();

@@ -218,6 +218,9 @@ struct VolPairs {
   // all flux pairs of element e: this warp's half of the volume columns and of
   // the face nodes; rows into acc (registers), face rows into the element's
   // face accumulators
+  // SMALL: every pair of the warp's elements has u < SMALL_U (small_pairs),
+  // so the fluxes take the u^2 series without a vote
+  template <bool SMALL>
   __device__ __forceinline__ void pairs(double (&acc)[R][Nf], const Phys &P) const {
     const double *st = sSt + e * SE;
     double *acc_f = sAcc + e * SA;
@@ -259,7 +262,7 @@ struct VolPairs {
           nv[r][d] = v;
         }
       }
-      ecflux_n_warp_hR<DIM, R>(A, B, nv, P, F);
+      ecflux_n_warp_hR<DIM, R, SMALL>(A, B, nv, P, F);
 #pragma unroll
       for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -302,7 +305,7 @@ struct VolPairs {
           for (int d = 0; d < DIM; ++d) nvr[r][d] = nv[d];
         }
       }
-      ecflux_n_warp_hR<DIM, R>(A, B, nvr, P, F);
+      ecflux_n_warp_hR<DIM, R, SMALL>(A, B, nvr, P, F);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const double w1 = w1h[(r * nfh + s) * L + l];
@@ -395,6 +398,14 @@ struct VolPairs {
 
   // warp 1 parks its partial rows in element e's state block ([Nf][Nq]);
   // call between two __syncthreads
+  // the pairs, with no per-pair vote where small_pairs allows
+  __device__ __forceinline__ void all_pairs(double (&acc)[R][Nf], const Phys &P) const {
+    if (small_pairs<DIM, NN, L>(sSt + e * SE, l))
+      pairs<true>(acc, P);
+    else
+      pairs<false>(acc, P);
+  }
+
   __device__ __forceinline__ void park_rows(const double (&acc)[R][Nf]) const {
     double *rowbuf = sSt + e * SE;
     if (h == 1) {
@@ -477,7 +488,7 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     gsync();
     if (PRE) prefetch_group(batch(ib + gridDim.x));  // the next batch's traces, during the pairs
     double acc[R][Nf];
-    v.pairs(acc, P);
+    v.all_pairs(acc, P);
     gsync();  // the group's pairs done: its state block becomes the row buffer
     if (SURF) {
       v.template surface<GT>(K, k0, q * G, tq, fgeo, mapPq, Qf, P);

@@ -11,9 +11,11 @@ lands each block directly in place.  Per LSRK stage: exchange, then the
 volume, surface and update kernels on the part's own elements.
 
 Only the surface kernel reads a neighbour's trace, so the exchange of stage s
-only has to finish before the surface kernel of stage s; per element, the
-kernels do the same arithmetic in any partition, so a partitioned run equals
-the single-domain run bit for bit.
+only has to finish before the surface kernel of stage s.  Per element the
+kernels do the same arithmetic in any partition, except for the volume
+kernel's per-warp choice of log-mean evaluation (which elements share a warp
+differs between a part and the whole mesh), so a partitioned run equals the
+single-domain run to rounding.
 """
 
 from __future__ import annotations

@@ -1,8 +1,9 @@
 """Partitioned runs on one GPU: the halo pack kernel (wadg_halo_pack) equals
 its host form bit for bit, and a mesh cut into 2-4 parts, each part stepping
 its own elements with the halo exchanged between stages (all parts in one
-process), gives the single-domain run's state bit for bit -- per element the
-kernels do the same arithmetic in any partition."""
+process), gives the single-domain run's state to rounding (the volume
+kernel's per-warp choice of log-mean evaluation depends on which elements
+share a warp)."""
 
 import numpy as np
 import pytest
@@ -68,7 +69,17 @@ def test_partitioned_run_equals_single_domain(cuda, name, nparts):
     got = PT.gather_Q(parts, geo.K)
     for p in parts:
         p.close()
-    assert np.array_equal(got, ref), float(np.abs(got - ref).max() / np.abs(ref).max())
+    assert _agree(got, ref), float(np.abs(got - ref).max() / np.abs(ref).max())
+
+
+def _agree(got, ref):
+    """The partitioned run equals the single-domain run to rounding (1e-12
+    relative, max norm): a part's elements share warps with other elements
+    than in the whole mesh, and the volume kernel picks its log-mean
+    evaluation per warp (the u^2 series without a vote where every pair of
+    the warp's elements is nearly equal), so a value can differ in its last
+    bit."""
+    return float(np.abs(got - ref).max() / np.abs(ref).max()) < 1e-12
 
 
 class _FakeAllToAll:
@@ -127,7 +138,7 @@ def test_run_dist_stream_ordering_with_a_fake_collective(cuda, monkeypatch):
     """run_dist (the overlapped exchange of partitioned multi-GPU runs) with
     two ranks as threads, each on its own stream, and the collective replaced
     by device copies on a third stream: the result equals the single-domain
-    run bit for bit, so pack -> exchange -> surface are ordered right."""
+    run to rounding, so pack -> exchange -> surface are ordered right."""
     import threading
 
     import torch.distributed as dist
@@ -172,4 +183,4 @@ def test_run_dist_stream_ordering_with_a_fake_collective(cuda, monkeypatch):
     got = PT.gather_Q(parts, geo.K)
     for p in parts:
         p.close()
-    assert np.array_equal(got, ref), float(np.abs(got - ref).max() / np.abs(ref).max())
+    assert _agree(got, ref), float(np.abs(got - ref).max() / np.abs(ref).max())
