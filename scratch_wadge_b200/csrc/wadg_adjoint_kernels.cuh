@@ -105,8 +105,11 @@ __device__ __forceinline__ void ibl_series(double isb, double fb, double F, doub
 // lane has u < 1e-6 for both means (nearly equal states, e.g. the whole
 // Taylor-Green field) the series are truncated at u^2 (remainders below
 // 1e-18 relative in the means and 1e-13 in their u-derivatives, which enter
-// multiplied by f < 1e-3)
-template <int DIM, bool WARP>
+// multiplied by f < 1e-3).  SMALL = true: the caller has established u <
+// SMALL_U (4e-6) for every pair of the warp's elements (small_pairs); the
+// truncated series without a vote (remainders below 1e-17 in the means and
+// 2e-11 in the derivatives, which enter multiplied by f < 2e-3).
+template <int DIM, bool WARP, bool SMALL = false>
 __device__ __forceinline__ FluxCore<DIM> flux_core(const AdjNode<DIM> &a, const AdjNode<DIM> &b) {
   FluxCore<DIM> k;
   const double sr = a.rho + b.rho, dr = a.rho - b.rho;
@@ -115,7 +118,7 @@ __device__ __forceinline__ FluxCore<DIM> flux_core(const AdjNode<DIM> &a, const 
   k.isb = rcp(sb);
   const double fr = dr * isr, fb = db * k.isb;
   const double ur = fr * fr, ub = fb * fb;
-  if (WARP && __all_sync(0xffffffffu, fmax(ur, ub) < 1e-6)) {
+  if (SMALL || (WARP && __all_sync(0xffffffffu, fmax(ur, ub) < 1e-6))) {
     rl_series(sr, fr, fma(fma(ur, -4.0 / 45.0, -1.0 / 3.0), ur, 1.0), fma(ur, -8.0 / 45.0, -1.0 / 3.0),
               k.rl, k.rla, k.rlb);
     ibl_series(k.isb, fb, fma(fma(ub, 1.0 / 5.0, 1.0 / 3.0), ub, 1.0), fma(ub, 2.0 / 5.0, 1.0 / 3.0),
@@ -190,11 +193,11 @@ __device__ __forceinline__ void flux_rev(const FluxCore<DIM> &k, const AdjNode<D
   }
 }
 
-template <int DIM, bool WARP>
+template <int DIM, bool WARP, bool SMALL = false>
 __device__ __forceinline__ void ecflux_vjp(const AdjNode<DIM> &a, const AdjNode<DIM> &b,
                                            const double *n, const double *c, const Phys &P,
                                            double *ba, double *bb) {
-  const FluxCore<DIM> k = flux_core<DIM, WARP>(a, b);
+  const FluxCore<DIM> k = flux_core<DIM, WARP, SMALL>(a, b);
   flux_rev<DIM, true>(k, a, b, n, c, P, ba, bb);
 }
 
@@ -498,6 +501,10 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
       for (int c = 0; c < NG; ++c) Ge[c] = nm[El::Nfaces * DIM + c];
     }
 
+    // the pair loops: with a vote per pair (SM = false) or, where every pair
+    // of the warp's elements is nearly equal (small_pairs), without
+    auto pair_loops = [&](auto small_tag) {
+    constexpr bool SM = decltype(small_tag)::value;
     // volume-volume pairs over this warp's column half
     {
       const int n_ = nv(h), j0 = cv(h);
@@ -526,7 +533,7 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
             }
             nvd[d] = v;
           }
-          ecflux_vjp<DIM, true>(A[r], B, nvd, cr[r], P, rb[r], cb);
+          ecflux_vjp<DIM, !SM, SM>(A[r], B, nvd, cr[r], P, rb[r], cb);
         }
 #pragma unroll
         for (int q = 0; q < NB; ++q) bar[q * NN + j] += cb[q];
@@ -571,13 +578,18 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
           double c[Nf];
 #pragma unroll
           for (int q = 0; q < Nf; ++q) c[q] = fma(w1, cr[r][q], w2 * cfs[q]);
-          ecflux_vjp<DIM, true>(A[r], B, nvd, c, P, rb[r], cb);
+          ecflux_vjp<DIM, !SM, SM>(A[r], B, nvd, c, P, rb[r], cb);
         }
 #pragma unroll
         for (int q = 0; q < NB; ++q) bar[q * NN + Nq + f] += cb[q];
         __syncwarp();
       }
     }
+    };
+    if (small_pairs<DIM, NN, L>(st, l))
+      pair_loops(BoolTag<true>());
+    else
+      pair_loops(BoolTag<false>());
     // row adjoints into the column adjoints, one warp of the element at a time
 #pragma unroll
     for (int hh = 0; hh < H; ++hh) {
