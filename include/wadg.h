@@ -559,14 +559,17 @@ int wadg_adjoint_create(wadg_app *app, int nsteps, int every,
                         wadg_adjoint **out);
 int wadg_adjoint_destroy(wadg_adjoint *adj);
 /* Forward run of nsteps steps of size dt from Q0 (copied into the app; the
- * projected traces are recomputed from it), storing the checkpoints.  The
- * app holds the final state Q(T) afterwards; QT (may be NULL) receives a
- * copy of it. */
+ * projected traces are recomputed from it), storing the checkpoints, and the
+ * stages of the last segment on its tape as they are computed (so that the
+ * reverse sweep need not recompute that segment).  The app holds the final
+ * state Q(T) afterwards; QT (may be NULL) receives a copy of it. */
 int wadg_adjoint_forward(wadg_adjoint *adj, const double *Q0, double dt,
                          double *QT);
 /* Reverse sweep: given QbarT = dJ/dQ(T), writes Qbar0 = dJ/dQ0 for the run
  * of the last wadg_adjoint_forward.  Recomputes each segment from its
- * checkpoint; leaves the app at Q(T). */
+ * checkpoint, except the last one while the forward run's tape of it is
+ * intact (always for the first sweep after a forward run; for later sweeps
+ * with at most two segments); leaves the app at Q(T). */
 int wadg_adjoint_reverse(wadg_adjoint *adj, const double *QbarT,
                          double *Qbar0);
 /* R(Q) = Minv rhs(u~(Q), uf~(Q)), the time derivative one stage applies

@@ -3,7 +3,8 @@
 // sweep walks the segments backwards, recomputes each segment's stages from
 // its checkpoint into a tape (Q and the projected traces u~, uf~ at the start
 // of every stage) and runs the stage adjoint kernels (wadg_adjoint_kernels.cuh)
-// over the tape in reverse order.  Recompute and adjoint run on two streams
+// over the tape in reverse order.  The last segment's tape is written by the
+// forward run itself, which computes those stages anyway.  Recompute and adjoint run on two streams
 // with two tapes, so that the adjoint of segment s overlaps the recompute of
 // segment s-1: the forward kernels fill the SMs the adjoint kernels leave
 // idle (the pair kernel's last wave, the small per-element kernels).
@@ -43,6 +44,10 @@ struct wadg_adjoint {
   double dt = 0.0;
   bool have_forward = false;
   double *ckpt = nullptr;                                      // (nseg + 1) x nv
+  // the tape of the last segment (tape (nseg - 1) % 2) holds its stages: the
+  // forward run writes it as it goes, so the reverse sweep need not
+  // recompute that segment
+  bool last_taped = false;
   // two tapes of 5*every stages: the VJP of one segment reads one while the
   // recompute of the previous segment fills the other
   double *tapeQ[2] = {nullptr, nullptr}, *tapeU[2] = {nullptr, nullptr},
@@ -264,6 +269,26 @@ void free_adj(wadg_adjoint *j) {
   if (j->vs) cudaStreamDestroy(j->vs);
 }
 
+// run n time steps of size dt from the app's current state on its stream,
+// taping (Q, u~, uf~) at the start of every stage into tape b; `last`: run
+// the final stage too (the forward run needs its result, a recompute not)
+int run_taped(wadg_adjoint *j, int n, int b, double dt, bool last) {
+  wadg_app *a = j->app;
+  cudaStream_t s = a->stream;
+  int r;
+  for (int t = 0; t < n; ++t)
+    for (int st = 0; st < 5; ++st) {
+      const size_t idx = (size_t)t * 5 + st;
+      if ((r = d2d(j->tapeQ[b] + idx * j->nv, a->Q, j->nv, s)) ||
+          (r = d2d(j->tapeU[b] + idx * j->nv, a->uq[a->cur], j->nv, s)) ||
+          (r = d2d(j->tapeUf[b] + idx * j->nf, a->uf[a->cur], j->nf, s)))
+        return r;
+      if (!last && t == n - 1 && st == 4) break;
+      if ((r = wadg_rk_step(a, RK4A[st], RK4B[st], dt))) return r;
+    }
+  return WADG_OK;
+}
+
 // recompute segment `seg` from its checkpoint on the app's stream, taping
 // (Q, u~, uf~) at the start of every stage into tape b
 int recompute(wadg_adjoint *j, int seg, int b) {
@@ -273,17 +298,7 @@ int recompute(wadg_adjoint *j, int seg, int b) {
   int r;
   if ((r = d2d(a->Q, j->ckpt + seg * j->nv, j->nv, s))) return r;
   if ((r = project(a, a->Q, a->uq[a->cur], a->uf[a->cur], a->resQ))) return r;
-  for (int t = 0; t < n; ++t)
-    for (int st = 0; st < 5; ++st) {
-      const size_t idx = (size_t)t * 5 + st;
-      if ((r = d2d(j->tapeQ[b] + idx * j->nv, a->Q, j->nv, s)) ||
-          (r = d2d(j->tapeU[b] + idx * j->nv, a->uq[a->cur], j->nv, s)) ||
-          (r = d2d(j->tapeUf[b] + idx * j->nf, a->uf[a->cur], j->nf, s)))
-        return r;
-      if (t == n - 1 && st == 4) break;  // the last stage's outputs are not needed
-      if ((r = wadg_rk_step(a, RK4A[st], RK4B[st], j->dt))) return r;
-    }
-  return WADG_OK;
+  return run_taped(j, n, b, j->dt, false);
 }
 
 }  // namespace
@@ -394,13 +409,22 @@ int wadg_adjoint_forward(wadg_adjoint *j, const double *Q0, double dt, double *Q
   wadg_app *a = j->app;
   cudaStream_t s = a->stream;
   int r;
+  j->last_taped = false;
   if ((r = d2d(a->Q, Q0, j->nv, s))) return r;
   if ((r = project(a, a->Q, a->uq[a->cur], a->uf[a->cur], a->resQ))) return r;
   for (int seg = 0; seg < j->nseg; ++seg) {
     if ((r = d2d(j->ckpt + seg * j->nv, a->Q, j->nv, s))) return r;
     const int n = std::min(j->every, j->nsteps - seg * j->every);
-    if ((r = wadg_rk_run(a, dt, n, 1))) return r;
+    // the last segment runs stage by stage into its tape (the states at the
+    // start of its stages are the ones a recompute from its checkpoint
+    // would produce, bit for bit); the others as graph-replayed steps
+    if (seg == j->nseg - 1)
+      r = run_taped(j, n, seg % 2, dt, true);
+    else
+      r = wadg_rk_run(a, dt, n, 1);
+    if (r) return r;
   }
+  j->last_taped = j->nseg > 0;
   if ((r = d2d(j->ckpt + j->nseg * j->nv, a->Q, j->nv, s))) return r;
   if (QT && (r = d2d(QT, a->Q, j->nv, s))) return r;
   j->dt = dt;
@@ -426,9 +450,13 @@ int wadg_adjoint_reverse(wadg_adjoint *j, const double *QbarT, double *Qbar0) {
   if ((r = ck(cudaMemsetAsync(j->resbar, 0, j->nv * sizeof(double), sv), "memset"))) return r;
   const int last = j->nseg - 1;
   if (last >= 0) {
-    if ((r = recompute(j, last, last % 2))) return r;
+    // the forward run taped the last segment, unless a reverse sweep since
+    // has refilled that tape with another segment
+    if (!j->last_taped && (r = recompute(j, last, last % 2))) return r;
     if ((r = ck(cudaEventRecord(j->evR[last % 2], sr), "event"))) return r;
   }
+  // with three segments or more, segment last - 2 refills the last one's tape
+  j->last_taped = j->nseg > 0 && j->nseg <= 2;
   for (int seg = last; seg >= 0; --seg) {
     const int b = seg % 2;
     const int n = std::min(j->every, j->nsteps - seg * j->every);

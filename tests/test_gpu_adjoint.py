@@ -183,6 +183,21 @@ def test_checkpoint_interval_does_not_change_the_gradient(cuda):
         assert np.array_equal(g, out[0])
 
 
+@pytest.mark.parametrize("every", [1, 4, 7])
+def test_repeated_reverse_sweeps_give_the_same_gradient(cuda, every):
+    """The first reverse sweep after a forward run reads the last segment
+    from the forward run's tape; later sweeps recompute it when another
+    segment has refilled that tape (7 steps: 7, 2 and 1 segments)"""
+    c, Q0, dt, nsteps = _run_case("tg3d_affine_N3", 7)
+    app = _app(c.geo, c.curved)
+    adj = Adjoint(app, nsteps, every)
+    QT = adj.forward(_dev(Q0), dt)
+    _, gT = rho2_objective(c.geo, QT)
+    g = [adj.reverse(gT).cpu().numpy() for _ in range(3)]
+    adj.close()
+    assert np.array_equal(g[1], g[0]) and np.array_equal(g[2], g[0])
+
+
 def test_run_function_autograd(cuda):
     """RunFunction: torch.autograd through the checkpointed run"""
     c, Q0, dt, nsteps = _run_case("vortex2d_curved_N3", 3)
