@@ -123,6 +123,14 @@ __device__ __forceinline__ FluxCore<DIM> flux_core(const AdjNode<DIM> &a, const 
               k.rl, k.rla, k.rlb);
     ibl_series(k.isb, fb, fma(fma(ub, 1.0 / 5.0, 1.0 / 3.0), ub, 1.0), fma(ub, 2.0 / 5.0, 1.0 / 3.0),
                k.ibl, k.ibla, k.iblb);
+  } else if (WARP && __all_sync(0xffffffffu, fmax(ur, ub) < 1e-2)) {
+    // every lane in the degree-8 series range for both means: the same
+    // series as below, with no per-lane branch
+    double G, dG, F, dF;
+    polyG_d(ur, G, dG);
+    rl_series(sr, fr, G, dG, k.rl, k.rla, k.rlb);
+    polyF_d(ub, F, dF);
+    ibl_series(k.isb, fb, F, dF, k.ibl, k.ibla, k.iblb);
   } else {
     if (ur < 1e-2) {
       double G, dG;

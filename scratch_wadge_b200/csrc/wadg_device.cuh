@@ -337,9 +337,11 @@ __device__ __forceinline__ bool small_pairs(const double *st, int l) {
 
 // ecflux_n_warp_h for R row states a[r] against one column state b: one
 // warp vote for all R pairs of every lane (the u^2 series when all of them
-// have u < 1e-6), then the R fluxes side by side -- independent chains in one
-// basic block, which the scheduler interleaves.  Same value per pair as
-// ecflux_n_warp_h to rounding.  Must be called by all 32 lanes of the warp.
+// have u < 1e-6; else the degree-8 series, without the per-lane choice of
+// the log-difference, when all of them have u < 1e-2), then the R fluxes side
+// by side -- independent chains in one basic block, which the scheduler
+// interleaves.  Same value per pair as ecflux_n_warp_h to rounding.  Must be
+// called by all 32 lanes of the warp.
 // SMALL = true: the caller has established u < SMALL_U for every pair
 // (small_pairs); the u^2 series, no vote.
 template <int DIM, int R, bool SMALL = false>
@@ -347,7 +349,7 @@ __device__ __forceinline__ void ecflux_n_warp_hR(const NodeState<DIM> (&a)[R], c
                                                  const double (&n)[R][DIM], const Phys &P,
                                                  double (&F)[R][DIM + 2]) {
   double hsr[R], dr[R], db[R], isb[R], ur[R], ub[R];
-  bool small = true;
+  bool small = true, mid = true;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const double sr = a[r].rho + b.rho, sb = a[r].beta + b.beta;
@@ -360,6 +362,7 @@ __device__ __forceinline__ void ecflux_n_warp_hR(const NodeState<DIM> (&a)[R], c
     ub[r] = fb * fb;
     hsr[r] = 0.5 * sr;
     small = small && fmax(ur[r], ub[r]) < 1e-6;
+    mid = mid && fmax(ur[r], ub[r]) < 1e-2;
   }
   double rl[R], ibl[R];
   if (SMALL || __all_sync(0xffffffffu, small)) {
@@ -367,6 +370,12 @@ __device__ __forceinline__ void ecflux_n_warp_hR(const NodeState<DIM> (&a)[R], c
     for (int r = 0; r < R; ++r) {
       rl[r] = hsr[r] * polyG2(ur[r]);
       ibl[r] = isb[r] * polyF2x2(ub[r]);
+    }
+  } else if (__all_sync(0xffffffffu, mid)) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      rl[r] = hsr[r] * polyG(ur[r]);
+      ibl[r] = isb[r] * polyFx2(ub[r]);
     }
   } else {
 #pragma unroll
