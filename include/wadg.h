@@ -71,10 +71,13 @@ int wadg_ctx_get_vol_warps(const wadg_ctx *ctx);
 /* Its node-to-thread map is a second axis: L lanes per element with R rows
  * each (by default about three rows per lane).  wadg_vol_shapes writes every
  * compiled (warps, rows) pair -- first those of wadg_vol_warps_candidates with
- * rows 0 (the default map), then the other maps where they fill the lanes
- * with less padding (2D N=4: 2 and 4 rows per lane for its 16 nodes) -- and
+ * rows 0 (the default map), then the maps with half or twice the lanes per
+ * element where they pad no more node slots, hold at most 4 rows per lane
+ * and fit 4 warps (2D N=4: 4 lanes x 4 rows; 3D N=1: 4 lanes x 1 row) -- and
  * returns their number (at most WADG_MAX_VOL_SHAPES);
- * wadg_ctx_set_vol_shape selects one (rows 0: as wadg_ctx_set_vol_warps). */
+ * wadg_ctx_set_vol_shape selects one (rows 0: as wadg_ctx_set_vol_warps).
+ * Results agree bit for bit across warp counts under one map and to
+ * rounding across maps. */
 #define WADG_MAX_VOL_SHAPES 5
 int wadg_vol_shapes(const wadg_ctx *ctx, int curved, int *warps, int *rows);
 int wadg_ctx_set_vol_shape(wadg_ctx *ctx, int curved, int warps, int rows);
