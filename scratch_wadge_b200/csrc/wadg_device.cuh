@@ -144,7 +144,9 @@ template <int DIM> struct NodeState {
 
 // from conservative variables q[f*stride]; beta = rho / (2p)
 // (Euler3Daffine.okl:22-26 pfun/beta, Euler2D.okl:19-21)
-template <int DIM>
+// LOGS = false: lrho and lbeta are left 0 (the caller fills them where the
+// log-difference branch of the log-mean may be taken)
+template <int DIM, bool LOGS = true>
 __device__ __forceinline__ NodeState<DIM> node_state(const double *q, int stride, const Phys &P) {
   NodeState<DIM> s;
   s.rho = q[0];
@@ -158,8 +160,8 @@ __device__ __forceinline__ NodeState<DIM> node_state(const double *q, int stride
   const double E = q[(DIM + 1) * stride];
   const double p = P.gm1 * (E - 0.5 * s.rho * kin);
   s.beta = 0.5 * s.rho * rcp(p);
-  s.lrho = log(s.rho);
-  s.lbeta = log(s.beta);
+  s.lrho = LOGS ? log(s.rho) : 0.0;
+  s.lbeta = LOGS ? log(s.beta) : 0.0;
   return s;
 }
 

@@ -124,14 +124,15 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
     const bool vact = k0 + q * G < K;
     if (vact) {
       gsync();  // the group's traces staged
-      v.prologue_range(K, k0, q * G, G, tq, GT, vgeo, vfgeo, uq, uf, P, PRE ? v.sPre : nullptr);
+      v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, uq, uf, P,
+                                       PRE ? v.sPre : nullptr);
       gsync();
     }
     const int knext = ib + gridDim.x < nb ? (ib + gridDim.x) * E : K;
     if (PRE) prefetch_group(knext);  // the next batch's traces, during the pairs
     if (vact) {
       double acc[R][Nf];
-      v.all_pairs(acc, P);
+      v.group_pairs(acc, P, q * G, tq, GT, gsync);
       gsync();
       v.template surface<GT>(K, k0, q * G, tq, fgeo, mapPq, uf, P);
       gsync();

@@ -151,7 +151,9 @@ struct VolPairs {
     prologue_range(K, k0, 0, E, tid, blockDim.x, vgeo, vfgeo, uq, uf, P, ufs);
   }
 
-  // the same for the batch elements [e0, e0 + ne), by threads t0, t0 + ts, ...
+  // the same for the batch elements [e0, e0 + ne), by threads t0, t0 + ts,
+  // ...; LOGS = false: without the per-node logarithms (fill_logs adds them)
+  template <bool LOGS = true>
   __device__ __forceinline__ void prologue_range(int K, int k0, int e0, int ne, int t0, int ts,
                                                  const double *vgeo, const double *vfgeo,
                                                  const double *uq, const double *uf,
@@ -164,15 +166,17 @@ struct VolPairs {
       const int kk = k - k0;
       const double *fsrc = (ufs && kk >= e0 && kk < e0 + ne) ? ufs + (size_t)kk * NF * Nf
                                                              : uf + (size_t)k * NF * Nf;
-      const NodeState<DIM> s = (n < Nq) ? node_state<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
-                                        : node_state<DIM>(fsrc + (n - Nq), NF, P);
+      const NodeState<DIM> s = (n < Nq) ? node_state<DIM, LOGS>(uq + (size_t)k * Nq * Nf + n, Nq, P)
+                                        : node_state<DIM, LOGS>(fsrc + (n - Nq), NF, P);
       double *st = sSt + ee * SE;
       st[0 * NN + n] = s.rho;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = 0.5 * s.vel[d];  // stored halved
       st[(DIM + 1) * NN + n] = s.beta;
-      st[(DIM + 2) * NN + n] = s.lrho;
-      st[(DIM + 3) * NN + n] = s.lbeta;
+      if (LOGS) {
+        st[(DIM + 2) * NN + n] = s.lrho;
+        st[(DIM + 3) * NN + n] = s.lbeta;
+      }
       if (CURVED) {  // geometric factors stored halved: a pair's average
                      // (G_i + G_j)/2 is then one addition, with the same bits
 #pragma unroll
@@ -398,12 +402,34 @@ struct VolPairs {
 
   // warp 1 parks its partial rows in element e's state block ([Nf][Nq]);
   // call between two __syncthreads
-  // the pairs, with no per-pair vote where small_pairs allows
-  __device__ __forceinline__ void all_pairs(double (&acc)[R][Nf], const Phys &P) const {
-    if (small_pairs<DIM, NN, L>(sSt + e * SE, l))
+  // the per-node logarithms of the batch elements [e0, e0 + ne) (threads t0,
+  // t0 + ts, ...), from the stored density and beta: the same values the
+  // prologue's node_state would have stored
+  __device__ __forceinline__ void fill_logs(int e0, int ne, int t0, int ts) const {
+    for (int t = t0; t < ne * NN; t += ts) {
+      double *st = sSt + (e0 + t / NN) * SE;
+      const int n = t % NN;
+      st[(DIM + 2) * NN + n] = log(st[n]);
+      st[(DIM + 3) * NN + n] = log(st[(DIM + 1) * NN + n]);
+    }
+  }
+
+  // The pair phase of the group (H warps, threads t0 .. t0 + ts - 1 over
+  // the batch elements [e0, e0 + G), `gsync` its barrier), after a prologue
+  // without logarithms: where every pair of the group's elements is nearly
+  // equal (small_pairs) the pairs take the u^2 series with no vote and need
+  // no logarithm; otherwise the logarithms are filled in first (they feed
+  // the log-difference branch).
+  template <typename Sync>
+  __device__ __forceinline__ void group_pairs(double (&acc)[R][Nf], const Phys &P, int e0, int t0,
+                                              int ts, Sync gsync) const {
+    if (small_pairs<DIM, NN, L>(sSt + e * SE, l)) {
       pairs<true>(acc, P);
-    else
+    } else {
+      fill_logs(e0, G, t0, ts);
+      gsync();
       pairs<false>(acc, P);
+    }
   }
 
   __device__ __forceinline__ void park_rows(const double (&acc)[R][Nf]) const {
@@ -484,11 +510,12 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     // group owning it may already have overwritten with its RHS
     if (k0 + q * G >= K) break;
     gsync();  // the group's traces staged / its previous batch done with its shared memory
-    v.prologue_range(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P, PRE ? v.sPre : nullptr);
+    v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P,
+                                     PRE ? v.sPre : nullptr);
     gsync();
     if (PRE) prefetch_group(batch(ib + gridDim.x));  // the next batch's traces, during the pairs
     double acc[R][Nf];
-    v.all_pairs(acc, P);
+    v.group_pairs(acc, P, q * G, tq, GT, gsync);
     gsync();  // the group's pairs done: its state block becomes the row buffer
     if (SURF) {
       v.template surface<GT>(K, k0, q * G, tq, fgeo, mapPq, Qf, P);
