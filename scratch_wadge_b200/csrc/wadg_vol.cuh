@@ -483,10 +483,9 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     else
       asm volatile("bar.sync %0, %1;\n" ::"r"(1 + q), "r"(GT) : "memory");
   };
-  // stage the group's elements of batch kb (face traces, a contiguous range
+  // stage the group's elements from kq on (face traces, a contiguous range
   // of Qf) into shared memory
-  auto prefetch_group = [&](int kb) {
-    const int kq = kb + q * G;
+  auto prefetch_group = [&](int kq) {
     if (kq < K) {
       const int n = min(K - kq, G) * NF * Nf;
       const double *src = Qf + (size_t)kq * NF * Nf;
@@ -496,24 +495,39 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     cp_async_commit();
   };
   __syncthreads();  // the tables are shared by every group
-  // the batches to run: all of them, or (a work list: the ensemble's active
-  // instances) the ascending batch indices blist[0 .. *nblist)
+  // The work: batches of E elements, all of them or (a work list: the
+  // ensemble's active instances) the ascending batch indices blist[0 ..
+  // *nblist), each cut into its NG group slices of G elements.  The groups
+  // take the slices independently: in round i group q of CTA b takes slice
+  // (i NG + q) grid + b, so a last, partial round leaves the busy groups
+  // spread over every SM (rather than whole CTAs busy and the other SMs
+  // idle).  Every slice is G consecutive elements, so the elements that
+  // share a warp, and the results, do not depend on the schedule.
+  constexpr int NG = W / H;
   const int nb = blist ? *nblist : (K + E - 1) / E;
-  auto batch = [&](int i) { return i < nb ? (blist ? blist[i] : i) * E : K; };
-  if (PRE) prefetch_group(batch(blockIdx.x));
+  const int ns = nb * NG, sstep = (int)gridDim.x * NG;
+  auto slice = [&](int g) {  // first element of slice g (K past the end)
+    if (g >= ns) return K;
+    const int cb = g / NG;
+    return (blist ? blist[cb] : cb) * E + (g - cb * NG) * G;
+  };
+  const int g0 = q * (int)gridDim.x + (int)blockIdx.x;
+  if (PRE) prefetch_group(slice(g0));
 
-  for (int ib = blockIdx.x; ib < nb; ib += gridDim.x) {
-    const int k0 = batch(ib);
+  for (int gi = g0; gi < ns; gi += sstep) {
+    const int kg = slice(gi);
     if (PRE) cp_async_wait_all();
-    // a group whose elements all lie past the end (the CTA's last batch) has
-    // nothing to compute, and must not read element K-1's input, which the
-    // group owning it may already have overwritten with its RHS
-    if (k0 + q * G >= K) break;
-    gsync();  // the group's traces staged / its previous batch done with its shared memory
+    // a slice whose elements all lie past the end (of a partial last batch)
+    // has nothing to compute, and must not read element K-1's input, which
+    // the group owning it may already have overwritten with its RHS
+    if (kg >= K) break;
+    // the helpers index the group's elements as k0 + q G + (0 .. G-1)
+    const int k0 = kg - q * G;
+    gsync();  // the group's traces staged / its previous slice done with its shared memory
     v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P,
                                      PRE ? v.sPre : nullptr);
     gsync();
-    if (PRE) prefetch_group(batch(ib + gridDim.x));  // the next batch's traces, during the pairs
+    if (PRE) prefetch_group(slice(gi + sstep));  // the next slice's traces, during the pairs
     double acc[R][Nf];
     v.group_pairs(acc, P, q * G, tq, GT, gsync);
     gsync();  // the group's pairs done: its state block becomes the row buffer
