@@ -183,14 +183,57 @@ adj_proj_mma_kernel(int K, const double *__restrict__ Jq, const double *__restri
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int k0 = blockIdx.x * EW, ne = min(EW, K - k0);
 
-  // ---- stage [vbar; vfbar] as X[k][f*8 + e] (rows beyond Nq + NF zero)
-  for (int t = threadIdx.x; t < EW * Nf * Nq; t += C::threads) {
-    const int e = t / (Nf * Nq), rem = t - e * (Nf * Nq), f = rem / Nq, n = rem - f * Nq;
-    X[n * LD + f * EW + e] = e < ne ? vbar[(size_t)k0 * Nf * Nq + t] : 0.0;
+  // ---- the epilogue's operands of the warp's (node, element) pairs, loaded
+  // first so that they arrive while the block is staged and multiplied
+  const int m = warp * 8 + (lane >> 2);
+  double Us[2][Nf], qbs[2][Nf], rbs[2][Nf], J[2];
+  if (warp < MQ) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int e = 2 * (lane & 3) + i;
+      const bool ok = m < Nq && e < ne;
+      const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
+      J[i] = ok ? Jq[(size_t)(k0 + e) * Nq + m] : 1.0;
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) {
+        Us[i][f] = ok ? Qs[id + f * Nq] : 1.0;
+        qbs[i][f] = ok ? Qbar[id + f * Nq] : 0.0;
+        rbs[i][f] = ok ? resbar[id + f * Nq] : 0.0;
+      }
+    }
   }
-  for (int t = threadIdx.x; t < EW * Nf * NF; t += C::threads) {
-    const int e = t / (Nf * NF), rem = t - e * (Nf * NF), f = rem / NF, n = rem - f * NF;
-    X[(Nq + n) * LD + f * EW + e] = e < ne ? vfbar[(size_t)k0 * Nf * NF + t] : 0.0;
+  // ---- stage [vbar; vfbar] as X[k][f*8 + e] (rows beyond Nq + NF zero):
+  // every load of the thread in flight before the stores
+  {
+    constexpr int T1N = EW * Nf * Nq, T2N = EW * Nf * NF;
+    constexpr int I1 = (T1N + C::threads - 1) / C::threads, I2 = (T2N + C::threads - 1) / C::threads;
+    double v1[I1], v2[I2];
+#pragma unroll
+    for (int it = 0; it < I1; ++it) {
+      const int t = threadIdx.x + it * C::threads;
+      v1[it] = (t < T1N && t / (Nf * Nq) < ne) ? vbar[(size_t)k0 * Nf * Nq + t] : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < I2; ++it) {
+      const int t = threadIdx.x + it * C::threads;
+      v2[it] = (t < T2N && t / (Nf * NF) < ne) ? vfbar[(size_t)k0 * Nf * NF + t] : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < I1; ++it) {
+      const int t = threadIdx.x + it * C::threads;
+      if (t < T1N) {
+        const int e = t / (Nf * Nq), rem = t - e * (Nf * Nq), f = rem / Nq, n = rem - f * Nq;
+        X[n * LD + f * EW + e] = v1[it];
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < I2; ++it) {
+      const int t = threadIdx.x + it * C::threads;
+      if (t < T2N) {
+        const int e = t / (Nf * NF), rem = t - e * (Nf * NF), f = rem / NF, n = rem - f * NF;
+        X[(Nq + n) * LD + f * EW + e] = v2[it];
+      }
+    }
   }
   for (int t = threadIdx.x; t < (KP1 - Nq - NF) * LD; t += C::threads) X[(Nq + NF) * LD + t] = 0.0;
   if (CURVED)
@@ -225,29 +268,24 @@ adj_proj_mma_kernel(int K, const double *__restrict__ Jq, const double *__restri
     }
   }
   // ---- adjoint of V(Q) and the LSRK adjoint update
-  double wn[2][Nf], J[2];
-  const int m = warp * 8 + (lane >> 2);
+  double wn[2][Nf];
   if (warp < MQ) {
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       const int e = 2 * (lane & 3) + i;
       const bool ok = m < Nq && e < ne;
       const size_t id = (size_t)(k0 + e) * Nq * Nf + m;
-      J[i] = ok ? Jq[(size_t)(k0 + e) * Nq + m] : 1.0;
 #pragma unroll
       for (int f = 0; f < Nf; ++f) wn[i][f] = 0.0;
       if (!ok) continue;
-      double U[Nf], x[Nf], Ub[Nf];
+      double x[Nf], Ub[Nf];
+#pragma unroll
+      for (int f = 0; f < Nf; ++f) x[f] = CURVED ? D[f][i] * J[i] : D[f][i];
+      adj::VU_vjp<DIM>(Us[i], x, gas_of(P), Ub);
 #pragma unroll
       for (int f = 0; f < Nf; ++f) {
-        U[f] = Qs[id + f * Nq];
-        x[f] = CURVED ? D[f][i] * J[i] : D[f][i];
-      }
-      adj::VU_vjp<DIM>(U, x, gas_of(P), Ub);
-#pragma unroll
-      for (int f = 0; f < Nf; ++f) {
-        const double qb = Qbar[id + f * Nq];
-        const double rt = fma(b_, qb, resbar[id + f * Nq]);
+        const double qb = qbs[i][f];
+        const double rt = fma(b_, qb, rbs[i][f]);
         const double rn = a_ * rt, qn = qb + Ub[f];
         resbar[id + f * Nq] = rn;
         Qbar[id + f * Nq] = qn;
