@@ -207,6 +207,89 @@ struct VolPairs {
     }
   }
 
+  // prologue_range for one element group: the G elements [e0, e0 + G) by
+  // TS threads t0, t0 + TS, ...; every conserved value the thread needs is
+  // loaded before any node state is computed, so the loads (global for the
+  // volume nodes) are in flight together rather than one node at a time
+  template <bool LOGS, int TS>
+  __device__ __forceinline__ void prologue_group(int K, int k0, int e0, int t0, const double *vgeo,
+                                                 const double *vfgeo, const double *uq,
+                                                 const double *uf, const Phys &P,
+                                                 const double *ufs) {
+    constexpr int NT = (G * NN + TS - 1) / TS;
+    // the thread's nodes in chunks of CH: a chunk's loads all in flight, few
+    // registers held
+    constexpr int CH = 2;
+#pragma unroll
+    for (int c0 = 0; c0 < NT; c0 += CH) {
+      double u[CH][Nf];
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        const int t = t0 + (c0 + j) * TS;
+        if (c0 + j < NT && t < G * NN) {
+          const int ee = e0 + t / NN, n = t % NN;
+          const int k = min(k0 + ee, K - 1);
+          // staged traces only for the group's own elements (a clamped
+          // element's copy may sit in another group's range)
+          const int kk = k - k0;
+          const double *fsrc = (ufs && kk >= e0 && kk < e0 + G) ? ufs + (size_t)kk * NF * Nf
+                                                               : uf + (size_t)k * NF * Nf;
+          const double *src = (n < Nq) ? uq + (size_t)k * Nq * Nf + n : fsrc + (n - Nq);
+          const int stride = (n < Nq) ? Nq : NF;
+#pragma unroll
+          for (int f = 0; f < Nf; ++f) u[j][f] = src[f * stride];
+        } else {
+#pragma unroll
+          for (int f = 0; f < Nf; ++f) u[j][f] = 1.0;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < CH; ++j) {
+        const int t = t0 + (c0 + j) * TS;
+        if (c0 + j < NT && t < G * NN) {
+          const int ee = e0 + t / NN, n = t % NN;
+          const int k = min(k0 + ee, K - 1);
+          const NodeState<DIM> s = node_state<DIM, LOGS>(u[j], 1, P);
+          double *st = sSt + ee * SE;
+          st[0 * NN + n] = s.rho;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = 0.5 * s.vel[d];  // stored halved
+          st[(DIM + 1) * NN + n] = s.beta;
+          if (LOGS) {
+            st[(DIM + 2) * NN + n] = s.lrho;
+            st[(DIM + 3) * NN + n] = s.lbeta;
+          }
+          if (CURVED) {  // geometric factors stored halved, as in prologue_range
+#pragma unroll
+            for (int c = 0; c < NG; ++c)
+              st[(NS + c) * NN + n] = 0.5 * ((n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
+                                                      : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)]);
+          }
+        }
+      }
+    }
+    for (int t = t0; t < G * SA; t += TS) sAcc[e0 * SA + t] = 0.0;
+    if (!CURVED) {
+      for (int t = e0 + t0; t < e0 + G; t += TS) {
+        const int k = min(k0 + t, K - 1);
+        double Gk[NG];
+#pragma unroll
+        for (int c = 0; c < NG; ++c) Gk[c] = vgeo[(size_t)k * Nq * NG + c * Nq];  // node 0 (:205)
+        double *nm = sNrm + t * SN;
+#pragma unroll
+        for (int c = 0; c < NG; ++c) nm[El::Nfaces * DIM + c] = Gk[c];
+        for (int fc = 0; fc < El::Nfaces; ++fc)
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            double v = 0.0;
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) v = fma(Gk[a * DIM + d], sNr[fc * DIM + a], v);
+            nm[fc * DIM + d] = v;
+          }
+      }
+    }
+  }
+
   // a node's state as the pair phase keeps it: velocity stored halved (u/2)
   __device__ __forceinline__ NodeState<DIM> load(const double *st, int n) const {
     NodeState<DIM> s;
@@ -524,8 +607,16 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     // the helpers index the group's elements as k0 + q G + (0 .. G-1)
     const int k0 = kg - q * G;
     gsync();  // the group's traces staged / its previous slice done with its shared memory
-    v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P,
-                                     PRE ? v.sPre : nullptr);
+    // the group prologue (every load of a chunk in flight first) is 2-7 %
+    // faster than the node-at-a-time one in the curved and 2D kernels; in
+    // the 3D affine volume + surface kernel it raised register spills (20 ->
+    // 64 bytes) and cost 2 %, so that one keeps prologue_range
+    if constexpr (SURF && DIM == 3 && !CURVED)
+      v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P,
+                                       PRE ? v.sPre : nullptr);
+    else
+      v.template prologue_group<false, GT>(K, k0, q * G, tq, vgeo, vfgeo, rhsQ, Qf, P,
+                                           PRE ? v.sPre : nullptr);
     gsync();
     if (PRE) prefetch_group(slice(gi + sstep));  // the next slice's traces, during the pairs
     double acc[R][Nf];
