@@ -414,30 +414,57 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     if (PRE) cp_async_wait_all();
     gsync();  // the group's traces staged / its previous batch done with its shared memory
     // ---- prologue: node states, face seeds, zeroed column adjoints, normals
-    for (int t = tq; t < G * NN; t += GT) {
-      const int ee = e0 + t / NN, n = t % NN;
-      const int k = min(k0 + ee, K - 1);
-      // staged traces only for the group's own elements (a clamped element's
-      // copy may sit in another group's range)
-      const int kk = k - k0;
-      const double *fsrc = (PRE && kk >= e0 && kk < e0 + G) ? sPre + (size_t)kk * NF * Nf
-                                                            : uf + (size_t)k * NF * Nf;
-      const AdjNode<DIM> s = (n < Nq) ? adj_node<DIM>(uq + (size_t)k * Nq * Nf + n, Nq, P)
-                                      : adj_node<DIM>(fsrc + (n - Nq), NF, P);
-      double *st = sEl + ee * C::per_elem;
-      st[0 * NN + n] = s.rho;
+    // (the thread's nodes in chunks of two, each chunk's loads in flight
+    // before its node states are computed)
+    {
+      constexpr int NT = (G * NN + GT - 1) / GT, CH = 2;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = s.vel[d];
-      st[(DIM + 1) * NN + n] = s.beta;
-      st[(DIM + 2) * NN + n] = s.lrho;
-      st[(DIM + 3) * NN + n] = s.lbeta;
-      st[(DIM + 4) * NN + n] = s.irho;
-      st[(DIM + 5) * NN + n] = s.ibeta;
-      if (CURVED) {
+      for (int c0 = 0; c0 < NT; c0 += CH) {
+        double u[CH][Nf];
 #pragma unroll
-        for (int c = 0; c < NG; ++c)
-          st[(NSA + c) * NN + n] = (n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
-                                            : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
+        for (int j = 0; j < CH; ++j) {
+          const int t = tq + (c0 + j) * GT;
+          if (c0 + j < NT && t < G * NN) {
+            const int ee = e0 + t / NN, n = t % NN;
+            const int k = min(k0 + ee, K - 1);
+            // staged traces only for the group's own elements (a clamped
+            // element's copy may sit in another group's range)
+            const int kk = k - k0;
+            const double *fsrc = (PRE && kk >= e0 && kk < e0 + G) ? sPre + (size_t)kk * NF * Nf
+                                                                  : uf + (size_t)k * NF * Nf;
+            const double *src = (n < Nq) ? uq + (size_t)k * Nq * Nf + n : fsrc + (n - Nq);
+            const int stride = (n < Nq) ? Nq : NF;
+#pragma unroll
+            for (int f = 0; f < Nf; ++f) u[j][f] = src[f * stride];
+          } else {
+#pragma unroll
+            for (int f = 0; f < Nf; ++f) u[j][f] = 1.0;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+          const int t = tq + (c0 + j) * GT;
+          if (c0 + j < NT && t < G * NN) {
+            const int ee = e0 + t / NN, n = t % NN;
+            const int k = min(k0 + ee, K - 1);
+            const AdjNode<DIM> s = adj_node<DIM>(u[j], 1, P);
+            double *st = sEl + ee * C::per_elem;
+            st[0 * NN + n] = s.rho;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = s.vel[d];
+            st[(DIM + 1) * NN + n] = s.beta;
+            st[(DIM + 2) * NN + n] = s.lrho;
+            st[(DIM + 3) * NN + n] = s.lbeta;
+            st[(DIM + 4) * NN + n] = s.irho;
+            st[(DIM + 5) * NN + n] = s.ibeta;
+            if (CURVED) {
+#pragma unroll
+              for (int c = 0; c < NG; ++c)
+                st[(NSA + c) * NN + n] = (n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
+                                                  : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)];
+            }
+          }
+        }
       }
     }
     for (int t = tq; t < G * C::SSF; t += GT) {
