@@ -222,8 +222,17 @@ __device__ __forceinline__ void UV(const double *V, double *U, const Phys &P) {
   const double h = 0.5 * vv * rcp(Vl);  // vv / (2 V_l)
   const double sV = P.gamma - V[0] + h;
   // rhoe = ((gamma-1)/(-V_l)^gamma)^(1/(gamma-1)) exp(-sV/(gamma-1)), as one
-  // exponential: exp((log(gamma-1) - gamma log(-V_l) - sV) / (gamma-1))
-  const double rhoe = exp((P.lgm1 - P.gamma * log(-Vl) - sV) * P.igm1);
+  // exponential: exp((log(gamma-1) - gamma log(-V_l) - sV) / (gamma-1)).
+  // For air (gamma = 1.4) the power is (-V_l)^(-7/2) = 1 / ((-V_l)^3
+  // sqrt(-V_l)): a square root and a reciprocal in place of the logarithm
+  // (within a few ulp of the general form)
+  double rhoe;
+  if (P.gamma == 1.4) {
+    const double mv = -Vl;
+    rhoe = exp((P.lgm1 - sV) * P.igm1) * rcp(mv * mv * mv * sqrt(mv));
+  } else {
+    rhoe = exp((P.lgm1 - P.gamma * log(-Vl) - sV) * P.igm1);
+  }
   U[0] = -rhoe * Vl;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) U[1 + d] = rhoe * V[1 + d];
