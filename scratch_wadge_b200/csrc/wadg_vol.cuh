@@ -208,10 +208,11 @@ struct VolPairs {
   }
 
   // prologue_range for one element group: the G elements [e0, e0 + G) by
-  // TS threads t0, t0 + TS, ...; every conserved value the thread needs is
-  // loaded before any node state is computed, so the loads (global for the
-  // volume nodes) are in flight together rather than one node at a time
-  template <bool LOGS, int TS>
+  // TS threads t0, t0 + TS, ...; a thread's nodes go in chunks of two whose
+  // loads (global for the volume nodes) are all issued before their node
+  // states are computed.  ROLLED: the chunks in a loop rather than unrolled
+  // (fewer registers live in a kernel that is short of them)
+  template <bool LOGS, int TS, bool ROLLED = false>
   __device__ __forceinline__ void prologue_group(int K, int k0, int e0, int t0, const double *vgeo,
                                                  const double *vfgeo, const double *uq,
                                                  const double *uf, const Phys &P,
@@ -220,7 +221,7 @@ struct VolPairs {
     // the thread's nodes in chunks of CH: a chunk's loads all in flight, few
     // registers held
     constexpr int CH = 2;
-#pragma unroll
+#pragma unroll(ROLLED ? 1 : NT)
     for (int c0 = 0; c0 < NT; c0 += CH) {
       double u[CH][Nf];
 #pragma unroll
@@ -609,11 +610,12 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     gsync();  // the group's traces staged / its previous slice done with its shared memory
     // the group prologue (every load of a chunk in flight first) is 2-7 %
     // faster than the node-at-a-time one in the curved and 2D kernels; in
-    // the 3D affine volume + surface kernel it raised register spills (20 ->
-    // 64 bytes) and cost 2 %, so that one keeps prologue_range
+    // the 3D affine volume + surface kernel its unrolled form raised register
+    // spills (20 -> 64 bytes) and cost 2 %, the rolled one (chunks in a loop)
+    // gains 1.5 %
     if constexpr (SURF && DIM == 3 && !CURVED)
-      v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, rhsQ, Qf, P,
-                                       PRE ? v.sPre : nullptr);
+      v.template prologue_group<false, GT, true>(K, k0, q * G, tq, vgeo, vfgeo, rhsQ, Qf, P,
+                                                 PRE ? v.sPre : nullptr);
     else
       v.template prologue_group<false, GT>(K, k0, q * G, tq, vgeo, vfgeo, rhsQ, Qf, P,
                                            PRE ? v.sPre : nullptr);
