@@ -124,13 +124,8 @@ stage_kernel(int K, const double *__restrict__ vgeo, const double *__restrict__ 
     const bool vact = k0 + q * G < K;
     if (vact) {
       gsync();  // the group's traces staged
-      // (the prologue choice of the volume + surface kernel)
-      if constexpr (DIM == 3 && !CURVED)
-        v.template prologue_range<false>(K, k0, q * G, G, tq, GT, vgeo, vfgeo, uq, uf, P,
-                                         PRE ? v.sPre : nullptr);
-      else
-        v.template prologue_group<false, GT>(K, k0, q * G, tq, vgeo, vfgeo, uq, uf, P,
-                                             PRE ? v.sPre : nullptr);
+      v.template prologue_group<false, GT>(K, k0, q * G, tq, vgeo, vfgeo, uq, uf, P,
+                                           PRE ? v.sPre : nullptr);
       gsync();
     }
     const int knext = ib + gridDim.x < nb ? (ib + gridDim.x) * E : K;

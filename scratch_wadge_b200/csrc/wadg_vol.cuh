@@ -142,77 +142,18 @@ struct VolPairs {
     }
   }
 
-  // node states of the batch (one thread per node); elements past the end
-  // replicate the last element so that every lane computes on valid data.
-  // ufs: the batch's face traces already staged in shared memory, or null
-  __device__ __forceinline__ void prologue(int K, int k0, const double *vgeo, const double *vfgeo,
-                                           const double *uq, const double *uf, const Phys &P,
-                                           const double *ufs = nullptr) {
-    prologue_range(K, k0, 0, E, tid, blockDim.x, vgeo, vfgeo, uq, uf, P, ufs);
-  }
-
-  // the same for the batch elements [e0, e0 + ne), by threads t0, t0 + ts,
-  // ...; LOGS = false: without the per-node logarithms (fill_logs adds them)
-  template <bool LOGS = true>
-  __device__ __forceinline__ void prologue_range(int K, int k0, int e0, int ne, int t0, int ts,
-                                                 const double *vgeo, const double *vfgeo,
-                                                 const double *uq, const double *uf,
-                                                 const Phys &P, const double *ufs) {
-    for (int t = t0; t < ne * NN; t += ts) {
-      const int ee = e0 + t / NN, n = t % NN;
-      const int k = min(k0 + ee, K - 1);
-      // staged traces only for this range's own elements (a clamped element's
-      // copy may sit in another range, staged by other threads)
-      const int kk = k - k0;
-      const double *fsrc = (ufs && kk >= e0 && kk < e0 + ne) ? ufs + (size_t)kk * NF * Nf
-                                                             : uf + (size_t)k * NF * Nf;
-      const NodeState<DIM> s = (n < Nq) ? node_state<DIM, LOGS>(uq + (size_t)k * Nq * Nf + n, Nq, P)
-                                        : node_state<DIM, LOGS>(fsrc + (n - Nq), NF, P);
-      double *st = sSt + ee * SE;
-      st[0 * NN + n] = s.rho;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) st[(1 + d) * NN + n] = 0.5 * s.vel[d];  // stored halved
-      st[(DIM + 1) * NN + n] = s.beta;
-      if (LOGS) {
-        st[(DIM + 2) * NN + n] = s.lrho;
-        st[(DIM + 3) * NN + n] = s.lbeta;
-      }
-      if (CURVED) {  // geometric factors stored halved: a pair's average
-                     // (G_i + G_j)/2 is then one addition, with the same bits
-#pragma unroll
-        for (int c = 0; c < NG; ++c)
-          st[(NS + c) * NN + n] = 0.5 * ((n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
-                                                  : vfgeo[(size_t)k * NF * NG + c * NF + (n - Nq)]);
-      }
-    }
-    for (int t = t0; t < ne * SA; t += ts) sAcc[e0 * SA + t] = 0.0;
-    if (!CURVED) {
-      for (int t = e0 + t0; t < e0 + ne; t += ts) {
-        const int k = min(k0 + t, K - 1);
-        double Gk[NG];
-#pragma unroll
-        for (int c = 0; c < NG; ++c) Gk[c] = vgeo[(size_t)k * Nq * NG + c * Nq];  // node 0 (:205)
-        double *nm = sNrm + t * SN;
-#pragma unroll
-        for (int c = 0; c < NG; ++c) nm[El::Nfaces * DIM + c] = Gk[c];
-        for (int fc = 0; fc < El::Nfaces; ++fc)
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            double v = 0.0;
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) v = fma(Gk[a * DIM + d], sNr[fc * DIM + a], v);
-            nm[fc * DIM + d] = v;
-          }
-      }
-    }
-  }
-
-  // prologue_range for one element group: the G elements [e0, e0 + G) by
-  // TS threads t0, t0 + TS, ...; a thread's nodes go in chunks of two whose
+  // Node states of one element group's batch elements [e0, e0 + G), by TS
+  // threads t0, t0 + TS, ...; elements past the end replicate the last
+  // element so that every lane computes on valid data.  ufs: the group's
+  // face traces already staged in shared memory, or null.  The states carry
+  // no logarithms unless LOGS (fill_logs adds them where a group needs
+  // them).  A thread's nodes go in chunks of two whose
   // loads (global for the volume nodes) are all issued before their node
-  // states are computed.  ROLLED: the chunks in a loop rather than unrolled
-  // (fewer registers live in a kernel that is short of them)
-  template <bool LOGS, int TS, bool ROLLED = false>
+  // states are computed.  The chunks run in a loop, not unrolled: unrolled,
+  // the 3D affine volume + surface kernel spilled registers (20 -> 64 bytes)
+  // and lost 2 %; rolled it gains 1.8 % there, 3 % in the affine volume
+  // kernel, and the same 2-7 % as unrolled in the curved and 2D kernels
+  template <bool LOGS, int TS>
   __device__ __forceinline__ void prologue_group(int K, int k0, int e0, int t0, const double *vgeo,
                                                  const double *vfgeo, const double *uq,
                                                  const double *uf, const Phys &P,
@@ -221,7 +162,7 @@ struct VolPairs {
     // the thread's nodes in chunks of CH: a chunk's loads all in flight, few
     // registers held
     constexpr int CH = 2;
-#pragma unroll(ROLLED ? 1 : NT)
+#pragma unroll 1
     for (int c0 = 0; c0 < NT; c0 += CH) {
       double u[CH][Nf];
 #pragma unroll
@@ -260,7 +201,8 @@ struct VolPairs {
             st[(DIM + 2) * NN + n] = s.lrho;
             st[(DIM + 3) * NN + n] = s.lbeta;
           }
-          if (CURVED) {  // geometric factors stored halved, as in prologue_range
+          if (CURVED) {  // geometric factors stored halved: a pair's average
+                         // (G_i + G_j)/2 is then one addition, with the same bits
 #pragma unroll
             for (int c = 0; c < NG; ++c)
               st[(NS + c) * NN + n] = 0.5 * ((n < Nq) ? vgeo[(size_t)k * Nq * NG + c * Nq + n]
@@ -608,17 +550,8 @@ vol_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     // the helpers index the group's elements as k0 + q G + (0 .. G-1)
     const int k0 = kg - q * G;
     gsync();  // the group's traces staged / its previous slice done with its shared memory
-    // the group prologue (every load of a chunk in flight first) is 2-7 %
-    // faster than the node-at-a-time one in the curved and 2D kernels; in
-    // the 3D affine volume + surface kernel its unrolled form raised register
-    // spills (20 -> 64 bytes) and cost 2 %, the rolled one (chunks in a loop)
-    // gains 1.5 %
-    if constexpr (SURF && DIM == 3 && !CURVED)
-      v.template prologue_group<false, GT, true>(K, k0, q * G, tq, vgeo, vfgeo, rhsQ, Qf, P,
-                                                 PRE ? v.sPre : nullptr);
-    else
-      v.template prologue_group<false, GT>(K, k0, q * G, tq, vgeo, vfgeo, rhsQ, Qf, P,
-                                           PRE ? v.sPre : nullptr);
+    v.template prologue_group<false, GT>(K, k0, q * G, tq, vgeo, vfgeo, rhsQ, Qf, P,
+                                         PRE ? v.sPre : nullptr);
     gsync();
     if (PRE) prefetch_group(slice(gi + sstep));  // the next slice's traces, during the pairs
     double acc[R][Nf];
