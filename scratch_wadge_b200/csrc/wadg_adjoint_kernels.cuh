@@ -414,11 +414,12 @@ adj_pairs_kernel(int K, const double *__restrict__ vgeo, const double *__restric
     if (PRE) cp_async_wait_all();
     gsync();  // the group's traces staged / its previous batch done with its shared memory
     // ---- prologue: node states, face seeds, zeroed column adjoints, normals
-    // (the thread's nodes in chunks of two, each chunk's loads in flight
-    // before its node states are computed)
+    // (the thread's nodes in chunks of four, each chunk's loads in flight
+    // before its node states are computed, the chunks in a rolled loop:
+    // reverse sweep 152.3 -> 148.0 ms at K=3072 against unrolled chunks of two)
     {
-      constexpr int NT = (G * NN + GT - 1) / GT, CH = 2;
-#pragma unroll
+      constexpr int NT = (G * NN + GT - 1) / GT, CH = 4;
+#pragma unroll 1
       for (int c0 = 0; c0 < NT; c0 += CH) {
         double u[CH][Nf];
 #pragma unroll
